@@ -1,0 +1,320 @@
+#!/usr/bin/env python
+"""RT orbital-updates/s of SALMON's 4th-order Taylor step on B200.
+
+Workload: the hpsi/Taylor operator microbench (cubic Si-like cell a=10.26 bohr,
+grid 32^3 by default, 4x4x4 = 64 k-points, 32 bands, 8 atoms x {s,p} Gaussian
+Kleinman-Bylander projectors, seeded synthetic orbitals and V_loc).  A step is
+one Taylor step of every orbital (4 H applications + the update).  Both orbital
+precisions run: complex(8) (FP64) and complex(4) orbitals with FP64
+reductions.  The headline `value` is the complex(4) path; the FP64 path is
+reported beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--grid 32] [--impl reference]
+
+Under torchrun (N>1) every rank propagates its own k-block of the same shape
+(weak scaling: fixed work per GPU, no collective in the timed Taylor loop; the
+end-to-end leg allreduces rho and J over NCCL like the reference's
+comm_summation).  Times are CUDA events on the library's stream, max over ranks.
+Inputs are larger than L2 (126 MB) at every pass, so no L2 flush is inserted.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RT orbital-updates/s: FP32+FP64-reduce vs FP64 GPU at ΔJ<1e-5; hpsi %HBM peak"
+DT = 0.08
+# ncu dram__bytes_{read,write}.sum of the stencil pass, per launch, from the
+# capture summarised in profiles/ (None until a capture exists for the config).
+NCU_TRAFFIC_BYTES = {}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--grid", type=int, default=32)
+    p.add_argument("--nkgrid", type=int, default=4)
+    p.add_argument("--nb", type=int, default=32)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def make_workload(args, rank):
+    from salmon_b200 import system as S
+    nk = args.nkgrid
+    return S.microbench_system(args.grid, nkgrid=(nk, nk, nk), Nb=args.nb, seed=S.SEED + rank)
+
+
+def cpu_baseline(sysm, kAc, vloc, zu, seconds):
+    """SALMON's own AVX stencil (compiled from the reference tree into oracle/_ref)
+    driving the Taylor step like RT/hamiltonian.f90, on all host cores, over a
+    bounded sample of the workload's orbitals."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        return None
+    _, zproj = O.update_projector(sysm, kAc)
+    nthreads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    chunk = max(nthreads * 4, 16)
+    # sample: the orbitals of the first k-points (at least `chunk` of them), propagated repeatedly
+    from salmon_b200 import system as S
+    sub = S.System(**{**{k: getattr(sysm, k) for k in ("NLx", "NLy", "NLz", "aL", "kAc0", "NB", "NBoccmax", "occ",
+                                                       "Rion", "Rps", "Mps", "Jxyz", "Jxx", "Jyy", "Jzz", "uV",
+                                                       "iuV", "a_tbl")}})
+    nkl = max(1, chunk // sysm.NBoccmax)
+    sub.NK_s, sub.NK_e = 1, nkl
+    za = O.aligned_state(zu[:nkl])
+    _, zp = O.update_projector(sub, kAc)
+    O.ref_hamiltonian(sub, kAc, vloc, zp, DT, za, nthreads=nthreads)  # warm-up
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        O.ref_hamiltonian(sub, kAc, vloc, zp, DT, za, nthreads=nthreads)
+        n += nkl * sysm.NBoccmax
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    return {"value": n / el, "unit": "orbital-updates/s", "cores": nthreads, "kind": "reference",
+            "sample": f"{nkl * sysm.NBoccmax} orbitals of the {sysm.NLx}^3 workload x {n // (nkl * sysm.NBoccmax)} "
+                      f"Taylor steps ({el:.1f} s); SALMON AVX hpsi1_rt_stencil_ + restated pseudo_pt/update, "
+                      f"OpenMP over orbitals, complex(8)"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    sysm, kAc, vloc, zu = make_workload(args, 0)
+    from oracle import oracle as O
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (SALMON AVX stencil build) missing"}))
+        return 0
+    secs = max(2.0, args.cpu_seconds / max(1, args.steps))
+    vals = []
+    for _ in range(args.warmup):
+        cpu_baseline(sysm, kAc, vloc, zu, 0.5)
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(sysm, kAc, vloc, zu, secs))
+    v = statistics.median(x["value"] for x in vals)
+    norb = sysm.nk_local * sysm.NBoccmax
+    out = {"metric": METRIC, "value": v, "unit": "orbital-updates/s", "n_gpus": 0, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1000.0 * norb / v, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+           "config": {"workload": f"hpsi/Taylor microbench {args.grid}^3, {sysm.NK} k x {sysm.NBoccmax} bands",
+                      "grid": args.grid, "nk": sysm.NK, "nb": sysm.NBoccmax},
+           "impl": "reference", "cpu_baseline": {k: vals[-1][k] for k in ("kind", "cores", "sample")} | {"value": v, "unit": "orbital-updates/s"},
+           "e2e": {"value": v, "unit": "orbital-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from salmon_b200 import build
+    build.build()
+    from salmon_b200.rt import GpuSystem
+
+    sysm, kAc, vloc, zu = make_workload(args, rank)
+    norb = sysm.nk_local * sysm.NBoccmax
+    NL = sysm.NL
+    hbm_peak, peak_kind = measured_peaks()
+    res = {}
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([x], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
+    clocks = None
+    for prec in ("c128", "c64"):
+        S_bytes = 16 if prec == "c128" else 8
+        g = GpuSystem(sysm, prec)
+        g.set_state(zu)
+        g.set_vloc(vloc)
+        g.update_projector(kAc)
+        stream = torch.cuda.ExternalStream(g.stream)
+        for _ in range(args.warmup):
+            g.hamiltonian(DT)
+        g.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        ctx = Clocks(local) if prec == "c64" else None
+        if ctx:
+            ctx.__enter__()
+        e0.record(stream)
+        for _ in range(args.steps):
+            g.hamiltonian(DT)
+        e1.record(stream)
+        e1.synchronize()
+        if ctx:
+            ctx.__exit__(None, None, None)
+            clocks = ctx.summary()
+        barrier()
+        torch.cuda.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        r = {"ms_per_step": ms / args.steps, "value": norb * world * args.steps / (ms / 1000.0)}
+        # dominant kernel: one H application of all orbitals (stencil + KB scatter), events on its stream
+        t_pass = g.time_kernel("stencil_pass", reps=10)
+        t_last = g.time_kernel("taylor_last", reps=5)
+        t_uv = g.time_kernel("uvpsi", reps=10)
+        alg = 2.0 * S_bytes * NL * norb  # algorithmic bytes of one H application over all orbitals
+        r.update(t_pass_ms=t_pass, t_last_ms=t_last, t_uvpsi_ms=t_uv, achieved_gbs=alg / (t_pass * 1e-3) / 1e9,
+                 step_gbs=10.0 * S_bytes * NL * norb / (r["ms_per_step"] * 1e-3) / 1e9)
+        # end to end through the C ABI with host buffers: k+A(t) and V_loc in, rho and J out, every step
+        kA = np.ascontiguousarray(kAc)
+        e0.record(stream)
+        for it in range(args.steps):
+            kt = kA + np.array([0.0, 0.0, 1e-4 * it])[:, None]
+            g.update_projector(kt)
+            g.set_vloc(vloc)
+            g.hamiltonian(DT)
+            rho = g.psi_rho_RT()
+            jav = g.current_RT(kt)
+            if world > 1:
+                import torch.distributed as dist
+                t = torch.from_numpy(np.concatenate([rho, jav])).cuda()
+                dist.all_reduce(t)
+                t.cpu()
+        e1.record(stream)
+        e1.synchronize()
+        ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+        r["e2e"] = {"value": norb * world * args.steps / (ms_e2e / 1000.0), "unit": "orbital-updates/s",
+                    "h2d_bytes_per_step": 2 * kA.nbytes + vloc.nbytes, "d2h_bytes_per_step": rho.nbytes + jav.nbytes}
+        res[prec] = r
+        g.close()
+        del stream
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            cpu = cpu_baseline(sysm, kAc, vloc, zu, args.cpu_seconds)
+        except Exception as exc:  # the CPU baseline is reported, never required
+            cpu = {"unavailable": str(exc)}
+    if rank == 0:
+        h = res["c64"]
+        traffic = NCU_TRAFFIC_BYTES.get(("stencil_pass", "c64", args.grid))
+        out = {
+            "metric": METRIC, "value": h["value"], "unit": "orbital-updates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": h["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c64 orbitals (FP32 stencil), FP64 reductions", "data": "synthetic",
+            "config": {"workload": f"hpsi/Taylor microbench {args.grid}^3, {sysm.NK} k x {sysm.NBoccmax} bands per GPU",
+                       "grid": args.grid, "nk": sysm.NK, "nb": sysm.NBoccmax, "norb_per_gpu": norb,
+                       "l2": "inputs larger than L2 at every pass (no flush)", "parallelism": f"k-blocks x{world}"},
+            "fp64_path": {"value": res["c128"]["value"], "ms_per_step": res["c128"]["ms_per_step"],
+                          "e2e": res["c128"]["e2e"], "stencil_pass_ms": res["c128"]["t_pass_ms"],
+                          "stencil_pass_gbs": res["c128"]["achieved_gbs"]},
+            "fp32_over_fp64": h["value"] / res["c128"]["value"],
+            "kernels_ms": {p: {"stencil_pass": res[p]["t_pass_ms"], "taylor_last": res[p]["t_last_ms"],
+                               "uvpsi": res[p]["t_uvpsi_ms"]} for p in res},
+            "step_gbs_algorithmic": {p: res[p]["step_gbs"] for p in res},
+            "roofline": {"bound": "hbm", "achieved": h["achieved_gbs"], "peak": hbm_peak, "unit": "GB/s",
+                         "frac": h["achieved_gbs"] / hbm_peak, "traffic": traffic,
+                         "kernel": "k_hpsi_pass<float,2,0> (one H application, all orbitals)",
+                         "peak_kind": peak_kind},
+            "cpu_baseline": cpu,
+            "e2e": h["e2e"],
+            "gpu_launches": args.steps * 8 * 1,
+            "clocks": clocks,
+        }
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

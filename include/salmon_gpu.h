@@ -1,0 +1,204 @@
+/*
+ * salmon_gpu.h -- C ABI of the B200 real-time propagation path for SALMON's
+ * periodic (ARTED) code.
+ *
+ * The entry points replace, one for one, the Fortran routines that SALMON 1.2.1
+ * calls on its real-time hot path.  Each declaration names the reference routine
+ * (file:line, paths relative to the SALMON source tree) whose argument meaning it
+ * keeps.  Arrays use the reference's Fortran (column-major) layout, so a Fortran
+ * caller passes its module arrays unchanged through ISO_C_BINDING:
+ *
+ *   zu(NL, NBoccmax, NK_s:NK_e)   complex(8)  orbital (ib,ik) is contiguous
+ *   grid index i = iz + NLz*(iy + NLy*ix)  (z is unit stride; init.f90:20-30)
+ *   kAc(NK, 3)                    real(8)     all k-points, column-major
+ *   occ(NB, NK)                   real(8)
+ *
+ * Conventions
+ *   - Every call returns 0 on success or a negative sgpu_status; it never aborts.
+ *     sgpu_last_error() returns a message for the last failure on this thread.
+ *     The Fortran shim maps non-zero to err_finalize (ARTED/main.f90:21-33).
+ *   - Pointers marked HOST are host memory; DEV are device memory of the
+ *     handle's device.  HOST arrays may be pageable or pinned.
+ *   - Calls on one handle are serialised on the handle's CUDA stream.  Calls
+ *     that return host results synchronise that stream; the rest are
+ *     asynchronous (sgpu_synchronize waits).  A handle must not be used from
+ *     two host threads at once.
+ *   - Orbitals stay resident on the device between calls, as the reference's
+ *     OpenACC build keeps zu_t resident (control/control_sc.f90:133-149).
+ */
+#ifndef SALMON_GPU_H
+#define SALMON_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+typedef enum sgpu_status {
+  SGPU_OK = 0,
+  SGPU_ERR_ARG = -1,      /* invalid argument or size                  */
+  SGPU_ERR_CUDA = -2,     /* CUDA runtime error (message has details)  */
+  SGPU_ERR_ALLOC = -3,    /* device allocation failed                  */
+  SGPU_ERR_STATE = -4,    /* call out of order (e.g. no state loaded)  */
+  SGPU_ERR_UNSUPPORTED = -5,
+  SGPU_ERR_TIMEOUT = -6   /* a bounded device wait gave up             */
+} sgpu_status;
+
+/* ---- precision modes (sgpu_set_precision) -------------------------------- */
+enum {
+  SGPU_PREC_C128 = 0,     /* complex(8) orbitals, FP64 everywhere                 */
+  SGPU_PREC_C64 = 1       /* complex(4) orbitals and stencils; FP64 reductions    */
+};
+
+/*
+ * System descriptor.  Mirrors the module data that ARTED builds in
+ * fd_coef (preparation/fd_coef.f90:20-83), init (preparation/init.f90:20-109),
+ * prep_ps_periodic (preparation/prep_ps.f90:80-204) and
+ * opt_vars_initialize_p2 (modules/opt_variables.f90:105-179).
+ * All pointer members are HOST and are copied by sgpu_create; the caller may
+ * free them afterwards.
+ */
+typedef struct sgpu_desc {
+  /* real-space grid (global_variables.f90:41-50) */
+  int32_t NLx, NLy, NLz;
+  double Hx, Hy, Hz;          /* grid spacing                          */
+  double aLx, aLy, aLz;       /* cell lengths                          */
+  /* k-points and bands */
+  int32_t NK;                 /* total k-points (first dim of kAc, second of occ) */
+  int32_t NK_s, NK_e;         /* 1-based k range held by this handle   */
+  int32_t NB;                 /* bands in occ (and in GS arrays)       */
+  int32_t NBoccmax;           /* occupied bands propagated in RT       */
+  /* Nd=4 finite-difference coefficients, already divided by H^2 and H
+   * (fd_coef.f90:75-80).  lap*[n] = lap(n) for n=0..4; nab*[n] = nab(n),
+   * nab*[0] is ignored. */
+  double lapx[5], lapy[5], lapz[5];
+  double nabx[5], naby[5], nabz[5];
+  /* Kleinman-Bylander nonlocal part (prep_ps.f90:80-204) */
+  int32_t NI;                 /* atoms                                  */
+  int32_t Nps;                /* max sphere points per atom             */
+  int32_t Nlma;               /* projectors in total                    */
+  const int32_t* Mps;         /* (NI)      sphere points of each atom   */
+  const int32_t* Jxyz;        /* (Nps,NI)  1-based grid index of point j of atom a */
+  const int32_t* Jxx;         /* (Nps,NI)  periodic image of the point  */
+  const int32_t* Jyy;         /* (Nps,NI)                               */
+  const int32_t* Jzz;         /* (Nps,NI)                               */
+  const double* uV;           /* (Nps,Nlma) projector values            */
+  const int32_t* iuV;         /* (Nlma)    sign of each projector       */
+  const int32_t* a_tbl;       /* (Nlma)    1-based atom of each projector */
+  const double* occ;          /* (NB,NK)   occupations                  */
+} sgpu_desc;
+
+typedef struct sgpu_system* sgpu_handle;
+
+/* ---- lifetime ------------------------------------------------------------ */
+
+/* Builds the device copies of every table in *desc on the current CUDA device
+ * and allocates the resident orbital array and Taylor workspace.
+ * Replaces: opt_vars_initialize_p2 + init_projector
+ * (modules/opt_variables.f90:105-179, :233-265) and the OpenACC
+ * `enter data` of control/control_sc.f90:133-149. */
+int sgpu_create(const sgpu_desc* desc, int precision, sgpu_handle* out);
+
+/* Frees every device buffer of the handle (opt_vars_finalize). */
+int sgpu_destroy(sgpu_handle h);
+
+/* Switches the orbital precision (SGPU_PREC_C128 or SGPU_PREC_C64).
+ * Resident orbitals are converted.  No reference counterpart: the reference
+ * propagates complex(8) only. */
+int sgpu_set_precision(sgpu_handle h, int precision);
+
+/* Message of the last failed call on this host thread (never NULL). */
+const char* sgpu_last_error(void);
+
+/* Waits for all work queued on the handle's stream. */
+int sgpu_synchronize(sgpu_handle h);
+
+/* The handle's cudaStream_t, for callers that time or order work around it. */
+void* sgpu_stream(sgpu_handle h);
+
+/* ---- resident state ------------------------------------------------------ */
+
+/* HOST zu(NL,NBoccmax,NK_s:NK_e) -> device.  Replaces the OpenACC
+ * `enter data copyin(zu_t)` / `update device(zu)` (control_sc.f90:149,
+ * RT/dt_evolve.f90:530). */
+int sgpu_set_state(sgpu_handle h, const double* zu /* complex(8), HOST */);
+
+/* device -> HOST zu.  Replaces `update self(zu_t)` (control_sc.f90:215,395,414). */
+int sgpu_get_state(sgpu_handle h, double* zu /* complex(8), HOST */);
+
+/* Device pointer of the resident orbitals (complex(8) or complex(4) per the
+ * precision), layout zu(NL,NBoccmax,NK_s:NK_e). */
+void* sgpu_state_ptr(sgpu_handle h);
+
+/* HOST Vloc(NL) -> device.  Vloc = Vh + Vpsl + Vexc (RT/dt_evolve.f90:206). */
+int sgpu_set_vloc(sgpu_handle h, const double* vloc);
+
+/* ---- hot path ------------------------------------------------------------ */
+
+/* Sets k+A(t) for the following hpsi/hamiltonian calls and rebuilds the
+ * k-dependent projectors zproj(j,ilma,ik) = conj(exp(i kAc.r)) uV(j,ilma).
+ * kAc is HOST (NK,3).  Replaces update_projector(kac) (common/projector.f90:29-115). */
+int sgpu_update_projector(sgpu_handle h, const double* kAc);
+
+/* One 4th-order Taylor step of every resident orbital:
+ *   zu <- zu + sum_{n=1..4} ((-i dt)^n / n!) H^n zu,
+ * with H built from the last sgpu_update_projector / sgpu_set_vloc.
+ * flag_current is accepted for argument compatibility and ignored (the
+ * reference ignores it unless built with ARTED_CURRENT_PREPROCESSING).
+ * Replaces hamiltonian(zu,flag_current) (RT/hamiltonian.f90:27-123). */
+int sgpu_hamiltonian(sgpu_handle h, double dt, int flag_current);
+
+/* H applied to one HOST orbital of k-point ik (1-based, NK_s<=ik<=NK_e).
+ * tpsi, htpsi are complex(8) (NL).  If ttpsi is not NULL it receives
+ * H tpsi - Vloc tpsi.  Replaces hpsi_omp_KB_GS / hpsi_omp_KB_RT
+ * (common/hpsi.f90:33-96). */
+int sgpu_hpsi(sgpu_handle h, int ik, const double* tpsi, double* htpsi, double* ttpsi);
+
+/* H applied to resident-layout DEV orbitals ikb_s..ikb_e (1-based over the
+ * (ib,ik) pairs of ik_table/ib_table, init.f90:101-109).  tpsi and htpsi
+ * point at orbital ikb_s of arrays laid out like zu, in the handle's
+ * precision.  Replaces hpsi_acc_KB_RT_LBLK (common/acc/hpsi.f90:28). */
+int sgpu_hpsi_batch(sgpu_handle h, int ikb_s, int ikb_e, const void* tpsi, void* htpsi);
+
+/* ---- reductions (FP64 in every precision mode) --------------------------- */
+
+/* rho_l(NL) = sum_{k,b} occ(b,k) |zu(:,b,k)|^2 over the resident orbitals,
+ * before the allreduce.  HOST output.  Replaces psi_rho_impl with Sym=1
+ * (common/psi_rho.f90:47-90, sym1 :181-206). */
+int sgpu_psi_rho(sgpu_handle h, double* rho_l);
+
+/* Macroscopic current of the resident orbitals at k+A = kAc (HOST (NK,3));
+ * jav(3) HOST, before the allreduce.  Rebuilds the projectors for kAc, as
+ * current() does.  Replaces current('RT',...) impl
+ * (RT/current.f90:78-292, current_stencil stencil/F90/current.f90:16-115). */
+int sgpu_current(sgpu_handle h, const double* kAc, double* jav);
+
+/* Kinetic and nonlocal energies of the resident orbitals at kAc (HOST):
+ *   Ekin = sum occ (Hxyz <psi|T + kAc.nabla|psi> + |kAc|^2/2),
+ *   Enl  = sum occ |<uV e^{ikr}|psi>|^2 iuV.
+ * Replaces the Ekin_l / Enl_l part of Total_Energy_omp
+ * (common/total_energy.f90:113-203, stencil/F90/total_energy.f90:25-188). */
+int sgpu_energy_terms(sgpu_handle h, const double* kAc, double* ekin, double* enl);
+
+/* ---- instrumentation ----------------------------------------------------- */
+/* Kernels that sgpu_time_kernel can time. */
+enum {
+  SGPU_KERNEL_STENCIL_PASS = 0, /* one H application of every resident orbital (zu -> workspace)     */
+  SGPU_KERNEL_TAYLOR_LAST = 1,  /* the fused last Taylor pass (H application + update), on workspace */
+  SGPU_KERNEL_UVPSI = 2,        /* the Kleinman-Bylander projections of every resident orbital       */
+  SGPU_KERNEL_PSI_RHO = 3       /* the density reduction                                             */
+};
+
+/* Launches `kernel` reps times back to back on the handle's stream between two
+ * CUDA events and returns the mean device time per launch.  The resident
+ * orbitals are not modified.  Counterpart of the reference's per-kernel timers
+ * (misc/timer.f90:34-54, LOG_HPSI_STENCIL etc.), which time on the host. */
+int sgpu_time_kernel(sgpu_handle h, int kernel, int reps, double* ms_per_launch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SALMON_GPU_H */

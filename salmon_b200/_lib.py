@@ -1,0 +1,75 @@
+"""ctypes binding of libsalmon_b200.so (include/salmon_gpu.h).
+
+There is no fallback: if the CUDA library is missing or cannot be loaded the
+import of the binding raises, and every call that fails on the device raises
+SalmonGPUError with the library's message (the reference aborts through
+err_finalize, ARTED/main.f90:21-33)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from .system import SgpuDesc
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsalmon_b200.so")
+
+# symbol -> (restype, argtypes); the list is the ABI of include/salmon_gpu.h
+_vp, _dp, _ip = C.c_void_p, C.POINTER(C.c_double), C.c_int
+ABI = {
+    "sgpu_create": (C.c_int, [C.POINTER(SgpuDesc), _ip, C.POINTER(C.c_void_p)]),
+    "sgpu_destroy": (C.c_int, [_vp]),
+    "sgpu_set_precision": (C.c_int, [_vp, _ip]),
+    "sgpu_last_error": (C.c_char_p, []),
+    "sgpu_synchronize": (C.c_int, [_vp]),
+    "sgpu_stream": (C.c_void_p, [_vp]),
+    "sgpu_set_state": (C.c_int, [_vp, _vp]),
+    "sgpu_get_state": (C.c_int, [_vp, _vp]),
+    "sgpu_state_ptr": (C.c_void_p, [_vp]),
+    "sgpu_set_vloc": (C.c_int, [_vp, _vp]),
+    "sgpu_update_projector": (C.c_int, [_vp, _vp]),
+    "sgpu_hamiltonian": (C.c_int, [_vp, C.c_double, _ip]),
+    "sgpu_hpsi": (C.c_int, [_vp, _ip, _vp, _vp, _vp]),
+    "sgpu_hpsi_batch": (C.c_int, [_vp, _ip, _ip, _vp, _vp]),
+    "sgpu_psi_rho": (C.c_int, [_vp, _vp]),
+    "sgpu_current": (C.c_int, [_vp, _vp, _vp]),
+    "sgpu_energy_terms": (C.c_int, [_vp, _vp, _dp, _dp]),
+    "sgpu_time_kernel": (C.c_int, [_vp, _ip, _ip, _dp]),
+}
+
+KERNELS = {"stencil_pass": 0, "taylor_last": 1, "uvpsi": 2, "psi_rho": 3}
+
+_LIB = None
+
+
+class SalmonGPUError(RuntimeError):
+    """A C-ABI call returned a non-zero status."""
+
+    def __init__(self, call, code, msg):
+        super().__init__(f"{call} failed ({code}): {msg}")
+        self.code = code
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is not built: run `python -m salmon_b200.build` "
+                               "(the CUDA library is required; there is no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in ABI.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def check(name, rc):
+    if rc != 0:
+        raise SalmonGPUError(name, rc, lib().sgpu_last_error().decode())
+    return rc
+
+
+def call(name, *args):
+    return check(name, getattr(lib(), name)(*args))

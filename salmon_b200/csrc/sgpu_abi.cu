@@ -1,0 +1,518 @@
+// C ABI of the B200 RT-propagation library (include/salmon_gpu.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "sgpu_internal.cuh"
+
+using sgpu::System;
+
+namespace {
+
+thread_local std::string g_err = "no error";
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  return fail(e == cudaErrorMemoryAllocation ? SGPU_ERR_ALLOC : SGPU_ERR_CUDA,
+              std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+}
+
+#define CK(expr)                                          \
+  do {                                                    \
+    cudaError_t e_ = (expr);                              \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #expr);   \
+  } while (0)
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t n) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  return cudaMalloc((void**)p, n * sizeof(T));
+}
+
+template <typename T>
+cudaError_t upload(T** p, const T* h, size_t n, cudaStream_t st) {
+  cudaError_t e = dalloc(p, n);
+  if (e != cudaSuccess || n == 0) return e;
+  return cudaMemcpyAsync(*p, h, n * sizeof(T), cudaMemcpyHostToDevice, st);
+}
+
+void free_state_buffers(System* s) {
+  cudaFree(s->zu);
+  for (auto& t : s->tw) { cudaFree(t); t = nullptr; }
+  s->zu = nullptr;
+}
+
+int alloc_state_buffers(System* s) {
+  const size_t n = (size_t)s->norb * s->NL;
+  s->elem = s->prec == SGPU_PREC_C64 ? sizeof(float2) : sizeof(double2);
+  CK(cudaMalloc(&s->zu, n * s->elem));
+  for (auto& t : s->tw) CK(cudaMalloc(&t, n * s->elem));
+  return 0;
+}
+
+bool valid(sgpu_handle h) { return h != nullptr; }
+
+// kAc(NK,3) host -> [nkl][3] device of the handle's k range
+int set_kac(System* s, const double* kAc) {
+  std::vector<double> loc(3 * (size_t)s->nkl);
+  for (int kl = 0; kl < s->nkl; ++kl)
+    for (int d = 0; d < 3; ++d) loc[3 * kl + d] = kAc[(size_t)d * s->NK + (s->NK_s - 1 + kl)];
+  s->kAc_h.assign(kAc, kAc + 3 * (size_t)s->NK);
+  CK(cudaMemcpyAsync(s->kAc_d, loc.data(), loc.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  // the staging vector must outlive the async copy
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int one_orbital_k(const System* s, int ik) { return (ik - s->NK_s) * s->NBocc; }
+
+}  // namespace
+
+struct sgpu_system : public System {};
+
+extern "C" {
+
+const char* sgpu_last_error(void) { return g_err.c_str(); }
+
+int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
+  if (!d || !out) return fail(SGPU_ERR_ARG, "sgpu_create: null argument");
+  *out = nullptr;
+  if (precision != SGPU_PREC_C128 && precision != SGPU_PREC_C64)
+    return fail(SGPU_ERR_ARG, "sgpu_create: precision must be SGPU_PREC_C128 or SGPU_PREC_C64");
+  if (d->NLx < 1 || d->NLy < 1 || d->NLz < 1) return fail(SGPU_ERR_ARG, "sgpu_create: grid sizes must be positive");
+  if (d->NK < 1 || d->NK_s < 1 || d->NK_e < d->NK_s || d->NK_e > d->NK)
+    return fail(SGPU_ERR_ARG, "sgpu_create: need 1 <= NK_s <= NK_e <= NK");
+  if (d->NB < 1 || d->NBoccmax < 1 || d->NBoccmax > d->NB)
+    return fail(SGPU_ERR_ARG, "sgpu_create: need 1 <= NBoccmax <= NB");
+  if (d->NI < 0 || d->Nlma < 0 || d->Nps < 0 || (d->NI > 0 && d->Nlma > 0 && d->Nps < 1))
+    return fail(SGPU_ERR_ARG, "sgpu_create: bad NI/Nps/Nlma");
+  if (!d->occ) return fail(SGPU_ERR_ARG, "sgpu_create: occ is NULL");
+  if (d->Nlma > 0 && (!d->Mps || !d->Jxyz || !d->Jxx || !d->Jyy || !d->Jzz || !d->uV || !d->iuV || !d->a_tbl))
+    return fail(SGPU_ERR_ARG, "sgpu_create: projector tables missing");
+  const int rz = (d->NLz % 2 == 0) ? 2 : 1;
+  if ((long)d->NLy * (d->NLz / rz) > 512)
+    return fail(SGPU_ERR_UNSUPPORTED, "sgpu_create: NLy*NLz/" + std::to_string(rz) + " > 512 threads per plane");
+  const long NL = (long)d->NLx * d->NLy * d->NLz;
+  if (NL > (1L << 30)) return fail(SGPU_ERR_ARG, "sgpu_create: grid too large");
+
+  sgpu_system* s = new (std::nothrow) sgpu_system();
+  if (!s) return fail(SGPU_ERR_ALLOC, "sgpu_create: host allocation failed");
+  auto bail = [&](int rc) {
+    sgpu_destroy(s);
+    return rc;
+  };
+  cudaError_t e = cudaGetDevice(&s->dev);
+  if (e != cudaSuccess) { delete s; return cuda_fail(e, "cudaGetDevice"); }
+  e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { delete s; return cuda_fail(e, "cudaStreamCreate"); }
+
+  s->prec = precision;
+  s->NLx = d->NLx; s->NLy = d->NLy; s->NLz = d->NLz; s->NL = (int)NL;
+  s->NK = d->NK; s->NK_s = d->NK_s; s->NK_e = d->NK_e; s->nkl = d->NK_e - d->NK_s + 1;
+  s->NB = d->NB; s->NBocc = d->NBoccmax; s->norb = s->nkl * s->NBocc;
+  s->H[0] = d->Hx; s->H[1] = d->Hy; s->H[2] = d->Hz;
+  s->aL[0] = d->aLx; s->aL[1] = d->aLy; s->aL[2] = d->aLz;
+  s->Hxyz = d->Hx * d->Hy * d->Hz;
+  s->aLxyz = d->aLx * d->aLy * d->aLz;
+  for (int n = 0; n < 5; ++n) {
+    s->lap[0][n] = d->lapx[n]; s->lap[1][n] = d->lapy[n]; s->lap[2][n] = d->lapz[n];
+    s->nab[0][n] = d->nabx[n]; s->nab[1][n] = d->naby[n]; s->nab[2][n] = d->nabz[n];
+  }
+  s->NI = d->Nlma > 0 ? d->NI : 0;
+  s->Nps = d->Nlma > 0 ? d->Nps : 0;
+  s->Nlma = d->Nlma;
+  s->occ_h.assign(d->occ, d->occ + (size_t)d->NB * d->NK);
+
+  // ---- projector tables: packed index (init_projector, opt_variables.f90:233-265)
+  std::vector<int> atom_off(s->NI + 1, 0), idx_proj;
+  std::vector<double> rpos;
+  for (int a = 0; a < s->NI; ++a) {
+    const int m = d->Mps[a];
+    if (m < 0 || m > s->Nps) return bail(fail(SGPU_ERR_ARG, "sgpu_create: Mps out of range"));
+    atom_off[a + 1] = atom_off[a] + m;
+    for (int j = 0; j < m; ++j) {
+      const int gi = d->Jxyz[(size_t)a * s->Nps + j] - 1;
+      if (gi < 0 || gi >= s->NL) return bail(fail(SGPU_ERR_ARG, "sgpu_create: Jxyz out of range"));
+      idx_proj.push_back(gi);
+      const int lx = gi / (s->NLy * s->NLz), ly = (gi / s->NLz) % s->NLy, lz = gi % s->NLz;
+      rpos.push_back(lx * s->H[0] - d->Jxx[(size_t)a * s->Nps + j] * s->aL[0]);
+      rpos.push_back(ly * s->H[1] - d->Jyy[(size_t)a * s->Nps + j] * s->aL[1]);
+      rpos.push_back(lz * s->H[2] - d->Jzz[(size_t)a * s->Nps + j] * s->aL[2]);
+    }
+  }
+  s->NPI = atom_off[s->NI];
+  std::vector<int> lma_atom(s->Nlma), iuv(s->Nlma), lma_list;
+  std::vector<int4> items;
+  for (int l = 0; l < s->Nlma; ++l) {
+    const int a = d->a_tbl[l] - 1;
+    if (a < 0 || a >= s->NI) return bail(fail(SGPU_ERR_ARG, "sgpu_create: a_tbl out of range"));
+    lma_atom[l] = a;
+    iuv[l] = d->iuV[l];
+  }
+  for (int a = 0; a < s->NI; ++a) {  // projectors grouped by atom, chunks of <= 4
+    std::vector<int> mine;
+    for (int l = 0; l < s->Nlma; ++l)
+      if (lma_atom[l] == a) mine.push_back(l);
+    for (size_t c = 0; c < mine.size(); c += 4) {
+      const int cnt = (int)std::min<size_t>(4, mine.size() - c);
+      items.push_back(make_int4(a, (int)lma_list.size(), cnt, 0));
+      for (int q = 0; q < cnt; ++q) lma_list.push_back(mine[c + q]);
+    }
+  }
+  s->nitems = (int)items.size();
+  // inverse map: for each grid point the (ilma, j) pairs whose sphere holds it
+  std::vector<int> cnt(s->NL + 1, 0);
+  for (int l = 0; l < s->Nlma; ++l) {
+    const int a = lma_atom[l];
+    for (int j = 0; j < d->Mps[a]; ++j) cnt[idx_proj[atom_off[a] + j] + 1]++;
+  }
+  for (int i = 0; i < s->NL; ++i) cnt[i + 1] += cnt[i];
+  std::vector<int2> ent(cnt[s->NL]);
+  {
+    std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+    for (int l = 0; l < s->Nlma; ++l) {
+      const int a = lma_atom[l];
+      for (int j = 0; j < d->Mps[a]; ++j) {
+        const int gi = idx_proj[atom_off[a] + j];
+        ent[fill[gi]++] = make_int2(l * s->Nps + j, l);
+      }
+    }
+  }
+  s->ninv = (int)ent.size();
+  std::vector<double> uv((size_t)s->Nlma * s->Nps);
+  if (s->Nlma) std::memcpy(uv.data(), d->uV, uv.size() * sizeof(double));
+
+  // per-orbital occupations of the resident (ik, ib) pairs
+  std::vector<double> occo(s->norb);
+  for (int kl = 0; kl < s->nkl; ++kl)
+    for (int b = 0; b < s->NBocc; ++b) occo[kl * s->NBocc + b] = s->occ_h[(size_t)(s->NK_s - 1 + kl) * s->NB + b];
+
+  // ---- device buffers
+  int rc;
+  if ((rc = alloc_state_buffers(s)) != 0) return bail(rc);
+#define UP(ptr, vec) \
+  do { e = upload(&ptr, vec.data(), vec.size(), s->stream); if (e != cudaSuccess) return bail(cuda_fail(e, "upload " #ptr)); } while (0)
+  UP(s->idx_proj, idx_proj);
+  UP(s->atom_off, atom_off);
+  UP(s->rpos, rpos);
+  UP(s->items, items);
+  UP(s->lma_list, lma_list);
+  UP(s->iuV_d, iuv);
+  UP(s->lma_atom, lma_atom);
+  UP(s->uV_d, uv);
+  UP(s->inv_off, cnt);
+  UP(s->inv_ent, ent);
+  UP(s->occ_o, occo);
+#undef UP
+  const size_t nz = (size_t)s->nkl * s->Nlma * s->Nps;
+  if ((e = dalloc(&s->zproj64, nz)) != cudaSuccess) return bail(cuda_fail(e, "alloc zproj64"));
+  if ((e = dalloc(&s->zproj32, nz)) != cudaSuccess) return bail(cuda_fail(e, "alloc zproj32"));
+  if ((e = cudaMemsetAsync(s->zproj64, 0, std::max<size_t>(nz, 1) * sizeof(double2), s->stream)) != cudaSuccess)
+    return bail(cuda_fail(e, "memset zproj64"));
+  if ((e = cudaMemsetAsync(s->zproj32, 0, std::max<size_t>(nz, 1) * sizeof(float2), s->stream)) != cudaSuccess)
+    return bail(cuda_fail(e, "memset zproj32"));
+  if ((e = dalloc(&s->U, (size_t)s->norb * std::max(1, s->Nlma))) != cudaSuccess) return bail(cuda_fail(e, "alloc U"));
+  if ((e = dalloc(&s->Uw, (size_t)s->norb * std::max(1, s->Nlma) * 4)) != cudaSuccess)
+    return bail(cuda_fail(e, "alloc Uw"));
+  if ((e = dalloc(&s->kAc_d, 3 * (size_t)s->nkl)) != cudaSuccess) return bail(cuda_fail(e, "alloc kAc"));
+  if ((e = dalloc(&s->vloc64, s->NL)) != cudaSuccess) return bail(cuda_fail(e, "alloc vloc64"));
+  if ((e = dalloc(&s->vloc32, s->NL)) != cudaSuccess) return bail(cuda_fail(e, "alloc vloc32"));
+  const size_t nchunk = (s->norb + 63) / 64;
+  s->red_elems = std::max<size_t>({nchunk * s->NL, 4 * (size_t)s->norb + 64, (size_t)s->NL + 64});
+  if ((e = dalloc(&s->red, s->red_elems)) != cudaSuccess) return bail(cuda_fail(e, "alloc red"));
+  s->red_h_elems = (size_t)s->NL + 64;
+  if ((e = cudaMallocHost((void**)&s->red_h, s->red_h_elems * sizeof(double))) != cudaSuccess)
+    return bail(cuda_fail(e, "alloc pinned"));
+  s->stage_elems = std::max<size_t>((size_t)4 * s->NL, std::min<size_t>((size_t)1 << 22, (size_t)s->norb * s->NL));
+  if ((e = dalloc(&s->stage, s->stage_elems)) != cudaSuccess) return bail(cuda_fail(e, "alloc stage"));
+  // zero kAc until the caller sets one
+  std::vector<double> k0(3 * (size_t)s->nkl, 0.0);
+  if ((e = cudaMemcpyAsync(s->kAc_d, k0.data(), k0.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream)) !=
+      cudaSuccess)
+    return bail(cuda_fail(e, "init kAc"));
+  if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) return bail(cuda_fail(e, "sgpu_create sync"));
+  *out = s;
+  return 0;
+}
+
+int sgpu_destroy(sgpu_handle h) {
+  if (!h) return 0;
+  System* s = h;
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  free_state_buffers(s);
+  void* bufs[] = {s->vloc64, s->vloc32, s->occ_o, s->kAc_d, s->idx_proj, s->atom_off, s->rpos, s->items,
+                  s->lma_list, s->iuV_d, s->lma_atom, s->uV_d, s->zproj64, s->zproj32, s->inv_off, s->inv_ent,
+                  s->U, s->Uw, s->red, s->stage};
+  for (void* p : bufs) cudaFree(p);
+  if (s->red_h) cudaFreeHost(s->red_h);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete h;
+  return 0;
+}
+
+int sgpu_synchronize(sgpu_handle h) {
+  if (!valid(h)) return fail(SGPU_ERR_ARG, "null handle");
+  CK(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+void* sgpu_stream(sgpu_handle h) { return h ? (void*)h->stream : nullptr; }
+
+void* sgpu_state_ptr(sgpu_handle h) { return h ? h->zu : nullptr; }
+
+int sgpu_set_state(sgpu_handle h, const double* zu) {
+  if (!valid(h) || !zu) return fail(SGPU_ERR_ARG, "sgpu_set_state: null argument");
+  System* s = h;
+  const size_t n = (size_t)s->norb * s->NL;
+  if (s->prec == SGPU_PREC_C128) {
+    CK(cudaMemcpyAsync(s->zu, zu, n * sizeof(double2), cudaMemcpyHostToDevice, s->stream));
+  } else {
+    for (size_t off = 0; off < n; off += s->stage_elems) {
+      const size_t c = std::min(s->stage_elems, n - off);
+      CK(cudaMemcpyAsync(s->stage, zu + 2 * off, c * sizeof(double2), cudaMemcpyHostToDevice, s->stream));
+      CK(sgpu::launch_c128_to_c64(s->stage, (float2*)s->zu + off, c, s->stream));
+    }
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  s->have_state = true;
+  return 0;
+}
+
+int sgpu_get_state(sgpu_handle h, double* zu) {
+  if (!valid(h) || !zu) return fail(SGPU_ERR_ARG, "sgpu_get_state: null argument");
+  System* s = h;
+  if (!s->have_state) return fail(SGPU_ERR_STATE, "sgpu_get_state: no state loaded");
+  const size_t n = (size_t)s->norb * s->NL;
+  if (s->prec == SGPU_PREC_C128) {
+    CK(cudaMemcpyAsync(zu, s->zu, n * sizeof(double2), cudaMemcpyDeviceToHost, s->stream));
+  } else {
+    for (size_t off = 0; off < n; off += s->stage_elems) {
+      const size_t c = std::min(s->stage_elems, n - off);
+      CK(sgpu::launch_c64_to_c128((const float2*)s->zu + off, s->stage, c, s->stream));
+      CK(cudaMemcpyAsync(zu + 2 * off, s->stage, c * sizeof(double2), cudaMemcpyDeviceToHost, s->stream));
+    }
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int sgpu_set_precision(sgpu_handle h, int precision) {
+  if (!valid(h)) return fail(SGPU_ERR_ARG, "null handle");
+  if (precision != SGPU_PREC_C128 && precision != SGPU_PREC_C64) return fail(SGPU_ERR_ARG, "bad precision");
+  System* s = h;
+  if (precision == s->prec) return 0;
+  const size_t n = (size_t)s->norb * s->NL;
+  void* old = s->zu;
+  const int old_prec = s->prec;
+  for (auto& t : s->tw) { cudaFree(t); t = nullptr; }
+  s->zu = nullptr;
+  s->prec = precision;
+  s->elem = precision == SGPU_PREC_C64 ? sizeof(float2) : sizeof(double2);
+  CK(cudaMalloc(&s->zu, n * s->elem));
+  if (s->have_state) {
+    if (old_prec == SGPU_PREC_C128)
+      CK(sgpu::launch_c128_to_c64((const double2*)old, (float2*)s->zu, n, s->stream));
+    else
+      CK(sgpu::launch_c64_to_c128((const float2*)old, (double2*)s->zu, n, s->stream));
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  cudaFree(old);
+  for (auto& t : s->tw) CK(cudaMalloc(&t, n * s->elem));
+  if (s->have_proj) CK(sgpu::launch_update_projector(*s));
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int sgpu_set_vloc(sgpu_handle h, const double* vloc) {
+  if (!valid(h) || !vloc) return fail(SGPU_ERR_ARG, "sgpu_set_vloc: null argument");
+  System* s = h;
+  CK(cudaMemcpyAsync(s->vloc64, vloc, s->NL * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  CK(sgpu::launch_r64_to_r32(s->vloc64, s->vloc32, s->NL, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  s->have_vloc = true;
+  return 0;
+}
+
+int sgpu_update_projector(sgpu_handle h, const double* kAc) {
+  if (!valid(h) || !kAc) return fail(SGPU_ERR_ARG, "sgpu_update_projector: null argument");
+  System* s = h;
+  int rc = set_kac(s, kAc);
+  if (rc) return rc;
+  CK(sgpu::launch_update_projector(*s));
+  s->have_proj = true;
+  return 0;
+}
+
+int sgpu_hamiltonian(sgpu_handle h, double dt, int flag_current) {
+  (void)flag_current;
+  if (!valid(h)) return fail(SGPU_ERR_ARG, "null handle");
+  System* s = h;
+  if (!s->have_state || !s->have_vloc || !s->have_proj)
+    return fail(SGPU_ERR_STATE, "sgpu_hamiltonian: state, Vloc and projectors must be set first");
+  // zfac(n) = (-i dt)^n / n!   (RT/hamiltonian.f90:46-49)
+  double zr = 0.0, zi = -dt;
+  sgpu::PassIO io;
+  io.zfac[0][0] = zr; io.zfac[0][1] = zi;
+  for (int i = 2; i <= 4; ++i) {
+    const double pr = io.zfac[i - 2][0], pi = io.zfac[i - 2][1];
+    io.zfac[i - 1][0] = (pr * 0.0 - pi * (-dt)) / i;
+    io.zfac[i - 1][1] = (pr * (-dt) + pi * 0.0) / i;
+  }
+  const void* ins[4] = {s->zu, s->tw[0], s->tw[1], s->tw[2]};
+  for (int n = 0; n < 4; ++n) {
+    CK(sgpu::launch_uvpsi(*s, ins[n], 0, s->norb, true));
+    io.in = ins[n];
+    if (n < 3) {
+      io.out = s->tw[n];
+      CK(sgpu::launch_hpsi_pass(*s, 0, io, 0, s->norb));
+    } else {
+      io.out = nullptr;
+      io.t1 = s->tw[0];
+      io.t2 = s->tw[1];
+      io.zu = s->zu;
+      CK(sgpu::launch_hpsi_pass(*s, 2, io, 0, s->norb));
+    }
+  }
+  return 0;
+}
+
+int sgpu_hpsi(sgpu_handle h, int ik, const double* tpsi, double* htpsi, double* ttpsi) {
+  if (!valid(h) || !tpsi || !htpsi) return fail(SGPU_ERR_ARG, "sgpu_hpsi: null argument");
+  System* s = h;
+  if (ik < s->NK_s || ik > s->NK_e) return fail(SGPU_ERR_ARG, "sgpu_hpsi: ik outside NK_s..NK_e");
+  if (!s->have_vloc || !s->have_proj) return fail(SGPU_ERR_STATE, "sgpu_hpsi: Vloc and projectors must be set first");
+  const size_t NL = s->NL;
+  double2* in128 = s->stage;
+  double2* out128 = s->stage + NL;
+  double2* tt128 = s->stage + 2 * NL;
+  CK(cudaMemcpyAsync(in128, tpsi, NL * sizeof(double2), cudaMemcpyHostToDevice, s->stream));
+  sgpu::PassIO io;
+  const int ob = one_orbital_k(s, ik);
+  if (s->prec == SGPU_PREC_C64) {
+    // FP32 scratch inside the (unused between calls) Taylor workspace
+    float2* in32 = (float2*)s->tw[0];
+    float2* out32 = (float2*)s->tw[1];
+    float2* tt32 = (float2*)s->tw[2];
+    CK(sgpu::launch_c128_to_c64(in128, in32, NL, s->stream));
+    io.in = in32; io.out = out32; io.tt = tt32;
+    CK(sgpu::launch_uvpsi(*s, in32, ob, 1, true));
+    CK(sgpu::launch_hpsi_pass(*s, ttpsi ? 1 : 0, io, ob, 1));
+    CK(sgpu::launch_c64_to_c128(out32, out128, NL, s->stream));
+    if (ttpsi) CK(sgpu::launch_c64_to_c128(tt32, tt128, NL, s->stream));
+  } else {
+    io.in = in128; io.out = out128; io.tt = tt128;
+    CK(sgpu::launch_uvpsi(*s, in128, ob, 1, true));
+    CK(sgpu::launch_hpsi_pass(*s, ttpsi ? 1 : 0, io, ob, 1));
+  }
+  CK(cudaMemcpyAsync(htpsi, out128, NL * sizeof(double2), cudaMemcpyDeviceToHost, s->stream));
+  if (ttpsi) CK(cudaMemcpyAsync(ttpsi, tt128, NL * sizeof(double2), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int sgpu_hpsi_batch(sgpu_handle h, int ikb_s, int ikb_e, const void* tpsi, void* htpsi) {
+  if (!valid(h) || !tpsi || !htpsi) return fail(SGPU_ERR_ARG, "sgpu_hpsi_batch: null argument");
+  System* s = h;
+  if (ikb_s < 1 || ikb_e < ikb_s || ikb_e > s->norb) return fail(SGPU_ERR_ARG, "sgpu_hpsi_batch: bad ikb range");
+  if (!s->have_vloc || !s->have_proj) return fail(SGPU_ERR_STATE, "sgpu_hpsi_batch: Vloc and projectors must be set first");
+  const int nb = ikb_e - ikb_s + 1;
+  sgpu::PassIO io;
+  io.in = tpsi;
+  io.out = htpsi;
+  CK(sgpu::launch_uvpsi(*s, tpsi, ikb_s - 1, nb, true));
+  CK(sgpu::launch_hpsi_pass(*s, 0, io, ikb_s - 1, nb));
+  return 0;
+}
+
+int sgpu_psi_rho(sgpu_handle h, double* rho_l) {
+  if (!valid(h) || !rho_l) return fail(SGPU_ERR_ARG, "sgpu_psi_rho: null argument");
+  System* s = h;
+  if (!s->have_state) return fail(SGPU_ERR_STATE, "sgpu_psi_rho: no state loaded");
+  double* out = s->stage ? (double*)s->stage : nullptr;  // NL doubles fit in the stage buffer
+  CK(sgpu::launch_psi_rho(*s, out));
+  CK(cudaMemcpyAsync(s->red_h, out, s->NL * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  std::memcpy(rho_l, s->red_h, s->NL * sizeof(double));
+  return 0;
+}
+
+int sgpu_current(sgpu_handle h, const double* kAc, double* jav) {
+  if (!valid(h) || !kAc || !jav) return fail(SGPU_ERR_ARG, "sgpu_current: null argument");
+  System* s = h;
+  if (!s->have_state) return fail(SGPU_ERR_STATE, "sgpu_current: no state loaded");
+  int rc = sgpu_update_projector(h, kAc);  // current() rebuilds the projectors (current.f90:125)
+  if (rc) return rc;
+  double* out = (double*)s->stage;
+  CK(sgpu::launch_current(*s, out));
+  CK(cudaMemcpyAsync(s->red_h, out, 3 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  std::memcpy(jav, s->red_h, 3 * sizeof(double));
+  return 0;
+}
+
+int sgpu_energy_terms(sgpu_handle h, const double* kAc, double* ekin, double* enl) {
+  if (!valid(h) || !kAc || !ekin || !enl) return fail(SGPU_ERR_ARG, "sgpu_energy_terms: null argument");
+  System* s = h;
+  if (!s->have_state) return fail(SGPU_ERR_STATE, "sgpu_energy_terms: no state loaded");
+  int rc = sgpu_update_projector(h, kAc);  // Total_Energy_omp calls update_projector(kac) (:122)
+  if (rc) return rc;
+  double* out = (double*)s->stage;
+  CK(sgpu::launch_energy(*s, out));
+  CK(cudaMemcpyAsync(s->red_h, out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  *ekin = s->red_h[0];
+  *enl = s->red_h[1];
+  return 0;
+}
+
+int sgpu_time_kernel(sgpu_handle h, int kernel, int reps, double* ms_per_launch) {
+  if (!valid(h) || !ms_per_launch || reps < 1) return fail(SGPU_ERR_ARG, "sgpu_time_kernel: bad argument");
+  System* s = h;
+  if (!s->have_state || !s->have_vloc || !s->have_proj)
+    return fail(SGPU_ERR_STATE, "sgpu_time_kernel: state, Vloc and projectors must be set first");
+  sgpu::PassIO io;
+  io.zfac[0][1] = -1e-3;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  auto launch = [&]() -> cudaError_t {
+    switch (kernel) {
+      case SGPU_KERNEL_STENCIL_PASS:
+        io.in = s->zu; io.out = s->tw[0];
+        return sgpu::launch_hpsi_pass(*s, 0, io, 0, s->norb);
+      case SGPU_KERNEL_TAYLOR_LAST:  // reads tw[2], tw[0], tw[1] and updates tw[2] in place (zu untouched)
+        io.in = s->tw[0]; io.t1 = s->tw[1]; io.t2 = s->tw[1]; io.zu = s->tw[2];
+        return sgpu::launch_hpsi_pass(*s, 2, io, 0, s->norb);
+      case SGPU_KERNEL_UVPSI:
+        return sgpu::launch_uvpsi(*s, s->zu, 0, s->norb, true);
+      case SGPU_KERNEL_PSI_RHO:
+        return sgpu::launch_psi_rho(*s, (double*)s->stage);
+      default:
+        return cudaErrorInvalidValue;
+    }
+  };
+  cudaError_t err = launch();  // warm-up (and argument check)
+  if (err == cudaSuccess) err = cudaEventRecord(e0, s->stream);
+  for (int r = 0; r < reps && err == cudaSuccess; ++r) err = launch();
+  if (err == cudaSuccess) err = cudaEventRecord(e1, s->stream);
+  if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+  float ms = 0;
+  if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (err != cudaSuccess) return cuda_fail(err, "sgpu_time_kernel");
+  *ms_per_launch = ms / reps;
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,135 @@
+// Internal declarations of the B200 RT-propagation library (not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/salmon_gpu.h"
+
+namespace sgpu {
+
+// ---------------------------------------------------------------- complex --
+template <typename R> struct C2Of;
+template <> struct C2Of<float> { using type = float2; };
+template <> struct C2Of<double> { using type = double2; };
+template <typename R> using C2 = typename C2Of<R>::type;
+
+template <typename R> __host__ __device__ __forceinline__ C2<R> mk(R x, R y) { C2<R> c; c.x = x; c.y = y; return c; }
+template <typename T> __host__ __device__ __forceinline__ T cadd(T a, T b) { a.x += b.x; a.y += b.y; return a; }
+template <typename T> __host__ __device__ __forceinline__ T csub(T a, T b) { a.x -= b.x; a.y -= b.y; return a; }
+// a*b
+template <typename T> __host__ __device__ __forceinline__ T cmul(T a, T b) {
+  T c; c.x = a.x * b.x - a.y * b.y; c.y = a.x * b.y + a.y * b.x; return c;
+}
+// acc + a*b
+template <typename T> __host__ __device__ __forceinline__ T cfma(T a, T b, T acc) {
+  acc.x = fma(a.x, b.x, fma(-a.y, b.y, acc.x)); acc.y = fma(a.x, b.y, fma(a.y, b.x, acc.y)); return acc;
+}
+// acc + conj(a)*b
+template <typename T> __host__ __device__ __forceinline__ T cfmaj(T a, T b, T acc) {
+  acc.x = fma(a.x, b.x, fma(a.y, b.y, acc.x)); acc.y = fma(a.x, b.y, fma(-a.y, b.x, acc.y)); return acc;
+}
+
+__device__ __forceinline__ double2 to_d2(float2 a) { return make_double2(a.x, a.y); }
+__device__ __forceinline__ double2 to_d2(double2 a) { return a; }
+template <typename R> __device__ __forceinline__ C2<R> from_d2(double2 a);
+template <> __device__ __forceinline__ float2 from_d2<float>(double2 a) { return make_float2((float)a.x, (float)a.y); }
+template <> __device__ __forceinline__ double2 from_d2<double>(double2 a) { return a; }
+
+// ------------------------------------------------------------ the system --
+// Per-handle state: sizes, constants and device buffers.
+struct System {
+  int dev = 0;
+  cudaStream_t stream = nullptr;
+  int prec = SGPU_PREC_C128;
+
+  int NLx = 0, NLy = 0, NLz = 0, NL = 0;
+  int NK = 0, NK_s = 1, NK_e = 0, nkl = 0, NB = 0, NBocc = 0, norb = 0;
+  double H[3] = {0, 0, 0}, aL[3] = {0, 0, 0}, Hxyz = 0, aLxyz = 0;
+  double lap[3][5] = {}, nab[3][5] = {};
+  int NI = 0, Nps = 0, Nlma = 0, NPI = 0, nitems = 0, ninv = 0;
+
+  std::vector<double> occ_h;       // occ(NB,NK)
+  std::vector<double> kAc_h;       // last kAc (NK,3)
+  bool have_state = false, have_vloc = false, have_proj = false;
+
+  // resident orbitals and Taylor workspace (precision-dependent element size)
+  void* zu = nullptr;              // [norb][NL]
+  void* tw[3] = {nullptr, nullptr, nullptr};
+  size_t elem = 16;                // bytes per complex element
+
+  double* vloc64 = nullptr;        // [NL]
+  float* vloc32 = nullptr;         // [NL]
+  double* occ_o = nullptr;         // [norb] occupation of each resident orbital
+  double* kAc_d = nullptr;         // [nkl][3]
+
+  // Kleinman-Bylander tables (built like init_projector, opt_variables.f90:233-265)
+  int* idx_proj = nullptr;         // [NPI] 0-based grid index, atom by atom
+  int* atom_off = nullptr;         // [NI+1] packed offset of each atom's points
+  double* rpos = nullptr;          // [NPI][3] x,y,z relative to the atom image (projector.f90:61)
+  int4* items = nullptr;           // [nitems] {atom, first lma_list slot, count (<=4), 0}
+  int* lma_list = nullptr;         // [Nlma] projectors grouped by atom
+  int* iuV_d = nullptr;            // [Nlma]
+  int* lma_atom = nullptr;         // [Nlma]
+  double* uV_d = nullptr;          // [Nlma][Nps]
+  double2* zproj64 = nullptr;      // [nkl][Nlma][Nps]
+  float2* zproj32 = nullptr;       // [nkl][Nlma][Nps]   (C64 mode)
+  int* inv_off = nullptr;          // [NL+1] CSR of (ilma,j) pairs touching each grid point
+  int2* inv_ent = nullptr;         // [ninv] {ilma*Nps + j, ilma}
+  double2* U = nullptr;            // [norb][Nlma] projections <uV e^{ikr}|psi> (scaled)
+  double2* Uw = nullptr;           // [norb][Nlma][4] weighted projections for the current
+
+  // reduction scratch
+  double* red = nullptr;           // device scratch for partial sums
+  size_t red_elems = 0;
+  double* red_h = nullptr;         // pinned host mirror
+  size_t red_h_elems = 0;
+
+  // host<->device staging for one orbital / chunked conversions
+  double2* stage = nullptr;        // [stage_elems] complex(8)
+  size_t stage_elems = 0;
+
+  // tuning
+  int nslab = 1;                   // x-slabs per orbital in the stencil pass
+};
+
+// ------------------------------------------------------------ kernel API --
+// All launches go to s.stream.  Orbitals of a batch are resident indices
+// [o_beg, o_beg+nb); k-point of resident orbital o is o / NBocc.
+
+// U[b][ilma] = Hxyz * (scale_iuv ? iuV : 1) * sum_j conj(zproj(j,ilma,k)) in_b(J_a(j))
+cudaError_t launch_uvpsi(const System& s, const void* in, int o_beg, int nb, bool scale_iuv);
+
+// One H application: out = H in  (mode 0), with ttpsi (mode 1), or the last
+// Taylor pass (mode 2): zu = zu + z1 t1 + z2 t2 + z3 in + z4 H in.  U must hold
+// the projections of `in` (launch_uvpsi with scale_iuv=true).
+struct PassIO {
+  const void* in = nullptr;
+  void* out = nullptr;
+  void* tt = nullptr;
+  const void* t1 = nullptr;
+  const void* t2 = nullptr;
+  void* zu = nullptr;
+  double zfac[4][2] = {};
+};
+cudaError_t launch_hpsi_pass(const System& s, int mode, const PassIO& io, int o_beg, int nb);
+
+// zproj(j,ilma,k) = conj(exp(i kAc.r)) uV(j,ilma)  for the local k-points.
+cudaError_t launch_update_projector(const System& s);
+
+// Precision conversion of n complex elements.
+cudaError_t launch_c128_to_c64(const double2* src, float2* dst, size_t n, cudaStream_t st);
+cudaError_t launch_c64_to_c128(const float2* src, double2* dst, size_t n, cudaStream_t st);
+cudaError_t launch_r64_to_r32(const double* src, float* dst, size_t n, cudaStream_t st);
+
+// rho(NL) = sum_o occ_o |zu_o|^2 into red -> host
+cudaError_t launch_psi_rho(System& s, double* rho_dev);
+// per-orbital current terms and the final jav(3) (device)
+cudaError_t launch_current(System& s, double* jav_dev);
+// per-orbital kinetic and nonlocal energies summed (device, 2 doubles)
+cudaError_t launch_energy(System& s, double* e_dev);
+
+}  // namespace sgpu

@@ -1,0 +1,150 @@
+"""Host-side mirror of SALMON's RT hot-path routines over the C ABI.
+
+The methods keep the reference's names and argument meaning (paths relative to
+the SALMON source tree):
+
+  update_projector(kAc)        common/projector.f90:29      zproj for k+A(t)
+  hamiltonian(dt)              RT/hamiltonian.f90:27         4th-order Taylor step
+  hpsi_omp_KB_RT(ik, tpsi)     common/hpsi.f90:89            H psi, one orbital
+  hpsi_omp_KB_GS(ik, tpsi)     common/hpsi.f90:33            H psi and H psi - V psi
+  psi_rho_RT()                 common/psi_rho.f90:40         density (before allreduce)
+  current_RT(kAc)              RT/current.f90:65             current (before allreduce)
+  energy_terms(kAc)            common/total_energy.f90:113   Ekin, Enl
+
+Orbitals stay on the device between calls; numpy arrays follow
+salmon_b200.system conventions: zu is complex128 of shape (nk_local, NBoccmax, NL).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import SalmonGPUError, call
+
+PRECISIONS = {"c128": 0, "c64": 1}
+
+
+def _vp(a):
+    return C.c_void_p(a.ctypes.data)
+
+
+class GpuSystem:
+    """One handle of the CUDA library: a system's tables plus its resident orbitals."""
+
+    def __init__(self, sysm, precision: str = "c128"):
+        self.sysm = sysm
+        self._desc = sysm.desc()
+        self._h = C.c_void_p()
+        call("sgpu_create", C.byref(self._desc), PRECISIONS[precision], C.byref(self._h))
+        self.precision = precision
+
+    # ---- lifetime
+    def close(self):
+        if self._h:
+            _lib.lib().sgpu_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def stream(self) -> int:
+        return _lib.lib().sgpu_stream(self._h) or 0
+
+    def state_ptr(self) -> int:
+        return _lib.lib().sgpu_state_ptr(self._h) or 0
+
+    def synchronize(self):
+        call("sgpu_synchronize", self._h)
+
+    def set_precision(self, precision: str):
+        call("sgpu_set_precision", self._h, PRECISIONS[precision])
+        self.precision = precision
+
+    # ---- resident state
+    def set_state(self, zu):
+        s = self.sysm
+        zu = np.ascontiguousarray(zu, dtype=np.complex128)
+        if zu.shape != (s.nk_local, s.NBoccmax, s.NL):
+            raise ValueError(f"zu must have shape {(s.nk_local, s.NBoccmax, s.NL)}, got {zu.shape}")
+        call("sgpu_set_state", self._h, _vp(zu))
+
+    def get_state(self):
+        s = self.sysm
+        zu = np.empty((s.nk_local, s.NBoccmax, s.NL), np.complex128)
+        call("sgpu_get_state", self._h, _vp(zu))
+        return zu
+
+    def set_vloc(self, vloc):
+        v = np.ascontiguousarray(vloc, dtype=np.float64)
+        if v.shape != (self.sysm.NL,):
+            raise ValueError("Vloc must have shape (NL,)")
+        call("sgpu_set_vloc", self._h, _vp(v))
+
+    # ---- hot path
+    def update_projector(self, kAc):
+        k = np.ascontiguousarray(kAc, dtype=np.float64)
+        if k.shape != (3, self.sysm.NK):
+            raise ValueError("kAc must have shape (3, NK) (Fortran kAc(NK,3))")
+        call("sgpu_update_projector", self._h, _vp(k))
+
+    def hamiltonian(self, dt: float, flag_current: bool = False):
+        call("sgpu_hamiltonian", self._h, C.c_double(dt), int(flag_current))
+
+    def hpsi_omp_KB_RT(self, ik: int, tpsi):
+        t = np.ascontiguousarray(tpsi, dtype=np.complex128)
+        h = np.empty_like(t)
+        call("sgpu_hpsi", self._h, ik, _vp(t), _vp(h), None)
+        return h
+
+    def hpsi_omp_KB_GS(self, ik: int, tpsi):
+        t = np.ascontiguousarray(tpsi, dtype=np.complex128)
+        h = np.empty_like(t)
+        tt = np.empty_like(t)
+        call("sgpu_hpsi", self._h, ik, _vp(t), _vp(h), _vp(tt))
+        return h, tt
+
+    def hpsi_batch(self, ikb_s: int, ikb_e: int, tpsi_dev: int, htpsi_dev: int):
+        call("sgpu_hpsi_batch", self._h, ikb_s, ikb_e, C.c_void_p(tpsi_dev), C.c_void_p(htpsi_dev))
+
+    def time_kernel(self, kernel: str, reps: int = 10) -> float:
+        """Mean device milliseconds per launch of one library kernel (CUDA events on the library stream)."""
+        ms = C.c_double()
+        call("sgpu_time_kernel", self._h, _lib.KERNELS[kernel], reps, C.byref(ms))
+        return ms.value
+
+    # ---- reductions
+    def psi_rho_RT(self):
+        rho = np.empty(self.sysm.NL)
+        call("sgpu_psi_rho", self._h, _vp(rho))
+        return rho
+
+    def current_RT(self, kAc):
+        k = np.ascontiguousarray(kAc, dtype=np.float64)
+        jav = np.empty(3)
+        call("sgpu_current", self._h, _vp(k), _vp(jav))
+        return jav
+
+    def energy_terms(self, kAc):
+        k = np.ascontiguousarray(kAc, dtype=np.float64)
+        ek, en = C.c_double(), C.c_double()
+        call("sgpu_energy_terms", self._h, _vp(k), C.byref(ek), C.byref(en))
+        return ek.value, en.value
+
+
+__all__ = ["GpuSystem", "SalmonGPUError", "PRECISIONS"]

@@ -1,0 +1,393 @@
+"""Host-side description of one periodic (ARTED) system.
+
+Mirrors the module data SALMON builds before its real-time loop, with the same
+names and the same Fortran (column-major) layouts, so that arrays move between
+this package, the C ABI and a Fortran caller unchanged.  numpy arrays are kept
+in C order with the Fortran axes reversed, e.g. ``zu(NL,NBoccmax,NK_s:NK_e)`` is
+a C-order array of shape ``(nk_local, NBoccmax, NL)``.
+
+Reference routines restated here (paths relative to the SALMON source tree):
+  fd_coef            preparation/fd_coef.f90:20-83
+  uniform k grid     preparation/init.f90:283-300 (Sym=1)
+  occupations        preparation/init.f90:91-95
+  sphere points      atom/pp/prep_pp.f90:263-347 (calc_jxyz, iperiodic=3)
+  Jxyz linear index  preparation/prep_ps.f90:120
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+ND = 4  # global_variables.f90:41
+
+# Reduced coordinates of the 8-atom diamond Si cell used by SALMON's bulk Si
+# tests (testsuites/002_bulk_rt/inputfile, &atomic_red_coor).
+DIAMOND_RED = np.array(
+    [[0.00, 0.00, 0.00], [0.25, 0.25, 0.25], [0.50, 0.00, 0.50], [0.00, 0.50, 0.50],
+     [0.50, 0.50, 0.00], [0.75, 0.25, 0.75], [0.25, 0.75, 0.75], [0.75, 0.75, 0.25]])
+
+
+def fd_coef(nd: int = ND):
+    """Central-difference coefficients lap(-nd:nd), nab(-nd:nd) before scaling.
+
+    Same closed-form products as preparation/fd_coef.f90:26-73.
+    Returns two arrays indexed n + nd.
+    """
+    n = nd
+    lap = np.zeros(2 * n + 1)
+    nab = np.zeros(2 * n + 1)
+    s = 0.0
+    for i in range(-n, n + 1):
+        if i == 0:
+            continue
+        for j in range(-n, n + 1):
+            if j == i or j == 0:
+                continue
+            s += 1.0 / (i * j)
+    lap[n] = s
+    for j in range(1, n + 1):
+        t = 1.0
+        for i in range(-n, n + 1):
+            if i != j:
+                t *= (j - i)
+        s = 0.0
+        for k in range(-n, n + 1):
+            if k == j or k == 0:
+                continue
+            s0 = 1.0
+            for i in range(-n, n + 1):
+                if i in (k, j, 0):
+                    continue
+                s0 *= -i
+            s += s0
+        lap[n + j] = 2.0 * s / t
+        lap[n - j] = lap[n + j]
+    for j in range(1, n + 1):
+        t = 1.0
+        for i in range(-n, n + 1):
+            if i != j:
+                t *= (j - i)
+        s = 1.0
+        for i in range(-n, n + 1):
+            if i in (j, 0):
+                continue
+            s *= -i
+        nab[n + j] = s / t
+        nab[n - j] = -nab[n + j]
+    return lap, nab
+
+
+def uniform_k_grid(nkx: int, nky: int, nkz: int, bl):
+    """kAc(NK,3) of init_uniform_k_grid with Sym=1 (init.f90:288-300).
+
+    Returned C-order with shape (3, NK) (Fortran kAc(NK,3))."""
+    ks = []
+    for ix in range(1, nkx + 1):
+        for iy in range(1, nky + 1):
+            for iz in range(1, nkz + 1):
+                ks.append([-bl[0] / 2 + (ix - 0.5) * bl[0] / nkx,
+                           -bl[1] / 2 + (iy - 0.5) * bl[1] / nky,
+                           -bl[2] / 2 + (iz - 0.5) * bl[2] / nkz])
+    return np.ascontiguousarray(np.array(ks).T)
+
+
+class SgpuDesc(C.Structure):
+    """ctypes mirror of ``sgpu_desc`` (include/salmon_gpu.h)."""
+    _fields_ = [
+        ("NLx", C.c_int32), ("NLy", C.c_int32), ("NLz", C.c_int32),
+        ("Hx", C.c_double), ("Hy", C.c_double), ("Hz", C.c_double),
+        ("aLx", C.c_double), ("aLy", C.c_double), ("aLz", C.c_double),
+        ("NK", C.c_int32), ("NK_s", C.c_int32), ("NK_e", C.c_int32),
+        ("NB", C.c_int32), ("NBoccmax", C.c_int32),
+        ("lapx", C.c_double * 5), ("lapy", C.c_double * 5), ("lapz", C.c_double * 5),
+        ("nabx", C.c_double * 5), ("naby", C.c_double * 5), ("nabz", C.c_double * 5),
+        ("NI", C.c_int32), ("Nps", C.c_int32), ("Nlma", C.c_int32),
+        ("Mps", C.POINTER(C.c_int32)), ("Jxyz", C.POINTER(C.c_int32)),
+        ("Jxx", C.POINTER(C.c_int32)), ("Jyy", C.POINTER(C.c_int32)), ("Jzz", C.POINTER(C.c_int32)),
+        ("uV", C.POINTER(C.c_double)), ("iuV", C.POINTER(C.c_int32)),
+        ("a_tbl", C.POINTER(C.c_int32)), ("occ", C.POINTER(C.c_double)),
+    ]
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+@dataclass
+class System:
+    """Grid, k-points, occupations and Kleinman-Bylander tables of one system."""
+    NLx: int
+    NLy: int
+    NLz: int
+    aL: np.ndarray                      # (3,) cell lengths
+    kAc0: np.ndarray                    # (3, NK)  kAc0(NK,3)
+    NB: int
+    NBoccmax: int
+    occ: np.ndarray                     # (NK, NB) occ(NB,NK)
+    Rion: np.ndarray                    # (NI, 3)  Rion(3,NI)
+    Rps: float                          # projector sphere radius
+    Mps: np.ndarray                     # (NI,)
+    Jxyz: np.ndarray                    # (NI, Nps) 1-based
+    Jxx: np.ndarray
+    Jyy: np.ndarray
+    Jzz: np.ndarray
+    uV: np.ndarray                      # (Nlma, Nps)
+    iuV: np.ndarray                     # (Nlma,)
+    a_tbl: np.ndarray                   # (Nlma,) 1-based
+    NK_s: int = 1
+    NK_e: int = 0
+    extra: dict = field(default_factory=dict)
+
+    def __post_init__(self):
+        if self.NK_e == 0:
+            self.NK_e = self.NK
+
+    # ---- derived quantities (global_variables.f90) ----
+    @property
+    def NL(self):
+        return self.NLx * self.NLy * self.NLz
+
+    @property
+    def NK(self):
+        return self.kAc0.shape[1]
+
+    @property
+    def nk_local(self):
+        return self.NK_e - self.NK_s + 1
+
+    @property
+    def H(self):
+        return self.aL / np.array([self.NLx, self.NLy, self.NLz])
+
+    @property
+    def Hxyz(self):
+        h = self.H
+        return float(h[0] * h[1] * h[2])
+
+    @property
+    def aLxyz(self):
+        return float(self.aL[0] * self.aL[1] * self.aL[2])
+
+    @property
+    def NI(self):
+        return self.Mps.shape[0]
+
+    @property
+    def Nps(self):
+        return self.Jxyz.shape[1]
+
+    @property
+    def Nlma(self):
+        return self.uV.shape[0]
+
+    def lap_nab(self):
+        """lapx..nabz(0:4) scaled by 1/H^2 and 1/H (fd_coef.f90:75-80)."""
+        lap, nab = fd_coef()
+        h = self.H
+        out = {}
+        for d, ax in enumerate("xyz"):
+            out["lap" + ax] = lap[ND:] / h[d] ** 2
+            out["nab" + ax] = nab[ND:] / h[d]
+        return out
+
+    def grid_coords(self):
+        """Lx, Ly, Lz of every grid point (init.f90:20-30), 0-based index order."""
+        ix, iy, iz = np.meshgrid(np.arange(self.NLx), np.arange(self.NLy), np.arange(self.NLz), indexing="ij")
+        return ix.ravel(), iy.ravel(), iz.ravel()
+
+    def desc(self) -> SgpuDesc:
+        """Builds the C descriptor; the arrays it points to are owned by self."""
+        for name in ("Mps", "Jxyz", "Jxx", "Jyy", "Jzz", "iuV", "a_tbl"):
+            setattr(self, name, np.ascontiguousarray(getattr(self, name), dtype=np.int32))
+        for name in ("uV", "occ"):
+            setattr(self, name, np.ascontiguousarray(getattr(self, name), dtype=np.float64))
+        d = SgpuDesc()
+        d.NLx, d.NLy, d.NLz = self.NLx, self.NLy, self.NLz
+        d.Hx, d.Hy, d.Hz = (float(v) for v in self.H)
+        d.aLx, d.aLy, d.aLz = (float(v) for v in self.aL)
+        d.NK, d.NK_s, d.NK_e = self.NK, self.NK_s, self.NK_e
+        d.NB, d.NBoccmax = self.NB, self.NBoccmax
+        ln = self.lap_nab()
+        for key in ("lapx", "lapy", "lapz", "nabx", "naby", "nabz"):
+            arr = getattr(d, key)
+            for n in range(5):
+                arr[n] = float(ln[key][n])
+        d.NI, d.Nps, d.Nlma = self.NI, self.Nps, self.Nlma
+        d.Mps, d.Jxyz, d.Jxx, d.Jyy, d.Jzz = (_ip(self.Mps), _ip(self.Jxyz), _ip(self.Jxx), _ip(self.Jyy),
+                                              _ip(self.Jzz))
+        d.uV, d.iuV, d.a_tbl, d.occ = _dp(self.uV), _ip(self.iuV), _ip(self.a_tbl), _dp(self.occ)
+        self._desc_keepalive = d
+        return d
+
+    def sphere_positions(self):
+        """x,y,z of point j of atom a relative to the cell image, as used by
+        update_projector and current (projector.f90:61, current.f90:253-255).
+        Shape (NI, Nps, 3)."""
+        h = self.H
+        i = self.Jxyz - 1
+        lx = i // (self.NLy * self.NLz)
+        ly = (i // self.NLz) % self.NLy
+        lz = i % self.NLz
+        return np.stack([lx * h[0] - self.Jxx * self.aL[0],
+                         ly * h[1] - self.Jyy * self.aL[1],
+                         lz * h[2] - self.Jzz * self.aL[2]], axis=-1)
+
+
+def calc_jxyz(NLx, NLy, NLz, aL, Rion, Rps):
+    """Sphere points of every atom, in the order of calc_jxyz with nc=2
+    (atom/pp/prep_pp.f90:314-345): images ix,iy,iz in -2..2, then grid points in
+    index order.  Returns Mps (NI,), Jxyz (1-based), Jxx, Jyy, Jzz as (NI, Nps)
+    and the distance components (NI, Nps, 3) from the atom image."""
+    h = np.asarray(aL) / np.array([NLx, NLy, NLz])
+    ix, iy, iz = np.meshgrid(np.arange(NLx), np.arange(NLy), np.arange(NLz), indexing="ij")
+    mx, my, mz = ix.ravel(), iy.ravel(), iz.ravel()
+    per_atom = []
+    for a in range(Rion.shape[0]):
+        js, jx, jy, jz, dv = [], [], [], [], []
+        for ax in range(-2, 3):
+            for ay in range(-2, 3):
+                for az in range(-2, 3):
+                    tx = Rion[a, 0] + ax * aL[0]
+                    ty = Rion[a, 1] + ay * aL[1]
+                    tz = Rion[a, 2] + az * aL[2]
+                    x = mx * h[0] - tx
+                    y = my * h[1] - ty
+                    z = mz * h[2] - tz
+                    r = np.sqrt(x * x + y * y + z * z)
+                    sel = np.nonzero(r < Rps)[0]
+                    if sel.size:
+                        js.append(mz[sel] + 1 + NLz * my[sel] + NLy * NLz * mx[sel])
+                        jx.append(np.full(sel.size, ax)); jy.append(np.full(sel.size, ay))
+                        jz.append(np.full(sel.size, az))
+                        dv.append(np.stack([x[sel], y[sel], z[sel]], axis=1))
+        per_atom.append((np.concatenate(js), np.concatenate(jx), np.concatenate(jy), np.concatenate(jz),
+                         np.concatenate(dv)))
+    NI = Rion.shape[0]
+    Mps = np.array([p[0].size for p in per_atom], dtype=np.int32)
+    Nps = int(Mps.max())
+    Jxyz = np.zeros((NI, Nps), np.int32)
+    Jxx = np.zeros((NI, Nps), np.int32)
+    Jyy = np.zeros((NI, Nps), np.int32)
+    Jzz = np.zeros((NI, Nps), np.int32)
+    dist = np.zeros((NI, Nps, 3))
+    for a, (js, jx, jy, jz, dv) in enumerate(per_atom):
+        m = js.size
+        Jxyz[a, :m], Jxx[a, :m], Jyy[a, :m], Jzz[a, :m], dist[a, :m] = js, jx, jy, jz, dv
+    return Mps, Jxyz, Jxx, Jyy, Jzz, dist
+
+
+def gaussian_projectors(Mps, dist, Hxyz, rc=2.0):
+    """s + (px,py,pz) projectors per atom: radial exp(-r^2/rc^2) times 1, x, y, z,
+    each normalised so that sum_j uV^2 Hxyz = 1; iuV = +1 (s), -1 (p).  Projectors
+    are numbered atom by atom, as set_lma_tbl does."""
+    NI, Nps = dist.shape[:2]
+    uV = np.zeros((NI * 4, Nps))
+    iuV = np.zeros(NI * 4, np.int32)
+    a_tbl = np.zeros(NI * 4, np.int32)
+    for a in range(NI):
+        m = Mps[a]
+        d = dist[a, :m]
+        r2 = (d * d).sum(axis=1)
+        rad = np.exp(-r2 / rc ** 2)
+        for p, ang in enumerate([np.ones(m), d[:, 0], d[:, 1], d[:, 2]]):
+            v = rad * ang
+            v = v / np.sqrt((v * v).sum() * Hxyz)
+            uV[4 * a + p, :m] = v
+            iuV[4 * a + p] = 1 if p == 0 else -1
+            a_tbl[4 * a + p] = a + 1
+    return uV, iuV, a_tbl
+
+
+def periodic_gaussian_vloc(NLx, NLy, NLz, aL, centres, depth, width):
+    """V(r) = -sum_a D_a exp(-|r-R_a|^2/w_a^2) summed over the 27 nearest images."""
+    h = np.asarray(aL) / np.array([NLx, NLy, NLz])
+    ix, iy, iz = np.meshgrid(np.arange(NLx), np.arange(NLy), np.arange(NLz), indexing="ij")
+    r = np.stack([ix.ravel() * h[0], iy.ravel() * h[1], iz.ravel() * h[2]], axis=1)
+    v = np.zeros(r.shape[0])
+    for a in range(centres.shape[0]):
+        for ax in (-1, 0, 1):
+            for ay in (-1, 0, 1):
+                for az in (-1, 0, 1):
+                    c = centres[a] + np.array([ax, ay, az]) * aL
+                    d2 = ((r - c) ** 2).sum(axis=1)
+                    v -= depth[a] * np.exp(-d2 / width[a] ** 2)
+    return v
+
+
+def orthonormalise(zu, Hxyz):
+    """Orthonormalises the bands of every k-point under <a|b> = Hxyz sum conj(a) b
+    (Householder QR; the span equals that of Gram-Schmidt).  zu: (nk, nb, NL)."""
+    out = np.empty_like(zu)
+    for k in range(zu.shape[0]):
+        q, r = np.linalg.qr(zu[k].T)
+        ph = np.sign(np.real(np.diag(r)))
+        ph[ph == 0] = 1
+        out[k] = (q * ph).T / np.sqrt(Hxyz)
+    return out
+
+
+SEED = 20261203
+
+
+def microbench_system(N: int, nkgrid=(4, 4, 4), Nb: int = 32, A=(1e-2, 0.0, 0.0), a: float = 10.26,
+                      seed: int = SEED, with_orbitals: bool = True, nk_limit: int | None = None):
+    """The hpsi/Taylor operator microbench system: cubic cell a=10.26 bohr, grid
+    N^3, uniform k grid shifted by A, Nb bands, V_loc = 8 seeded periodic
+    Gaussians (depth U(0.5,2) Ha, width U(1,2) bohr) on the diamond sites,
+    8 atoms x {s,px,py,pz} Gaussian projectors (r_c = 2 bohr, R_ps = 2 bohr).
+
+    Returns (system, kAc (3,NK), Vloc (NL,), zu (nk,Nb,NL) complex128 or None).
+    ``nk_limit`` keeps only the first k-points (small test cases)."""
+    rng = np.random.default_rng(seed)
+    aL = np.array([a, a, a])
+    bl = 2 * np.pi / aL
+    kAc0 = uniform_k_grid(*nkgrid, bl)
+    if nk_limit is not None:
+        kAc0 = np.ascontiguousarray(kAc0[:, :nk_limit])
+    NK = kAc0.shape[1]
+    nkxyz = nkgrid[0] * nkgrid[1] * nkgrid[2]
+    occ = np.full((NK, Nb), 2.0 / nkxyz)
+    Rion = DIAMOND_RED * aL
+    Mps, Jxyz, Jxx, Jyy, Jzz, dist = calc_jxyz(N, N, N, aL, Rion, 2.0)
+    Hxyz = float(np.prod(aL / N))
+    uV, iuV, a_tbl = gaussian_projectors(Mps, dist, Hxyz)
+    depth = rng.uniform(0.5, 2.0, Rion.shape[0])
+    width = rng.uniform(1.0, 2.0, Rion.shape[0])
+    vloc = periodic_gaussian_vloc(N, N, N, aL, Rion, depth, width)
+    sysm = System(NLx=N, NLy=N, NLz=N, aL=aL, kAc0=kAc0, NB=Nb, NBoccmax=Nb, occ=occ, Rion=Rion, Rps=2.0,
+                  Mps=Mps, Jxyz=Jxyz, Jxx=Jxx, Jyy=Jyy, Jzz=Jzz, uV=uV, iuV=iuV, a_tbl=a_tbl)
+    sysm.extra.update(seed=seed, depth=depth, width=width)
+    kAc = np.ascontiguousarray(kAc0 + np.asarray(A, dtype=np.float64)[:, None])
+    zu = None
+    if with_orbitals:
+        NL = N ** 3
+        zu = rng.standard_normal((NK, Nb, NL)) + 1j * rng.standard_normal((NK, Nb, NL))
+        zu = orthonormalise(zu, Hxyz)
+    return sysm, kAc, vloc, zu
+
+
+def small_system(NLx=8, NLy=8, NLz=10, nk=3, nb=4, a=(6.0, 6.5, 7.0), nat=2, seed=7, Rps=1.6):
+    """A small non-cubic system with ragged sizes for exhaustive parity tests:
+    uneven grid, few k-points and bands, random atom sites, Gaussian projectors."""
+    rng = np.random.default_rng(seed)
+    aL = np.asarray(a, dtype=np.float64)
+    kAc0 = np.ascontiguousarray(rng.uniform(-0.5, 0.5, (3, nk)))
+    occ = rng.uniform(0.1, 1.0, (nk, nb))
+    Rion = rng.uniform(0, 1, (nat, 3)) * aL
+    Mps, Jxyz, Jxx, Jyy, Jzz, dist = calc_jxyz(NLx, NLy, NLz, aL, Rion, Rps)
+    Hxyz = float(np.prod(aL / np.array([NLx, NLy, NLz])))
+    uV, iuV, a_tbl = gaussian_projectors(Mps, dist, Hxyz, rc=Rps)
+    vloc = periodic_gaussian_vloc(NLx, NLy, NLz, aL, Rion, rng.uniform(0.5, 2, nat), rng.uniform(1, 2, nat))
+    sysm = System(NLx=NLx, NLy=NLy, NLz=NLz, aL=aL, kAc0=kAc0, NB=nb, NBoccmax=nb, occ=occ, Rion=Rion, Rps=Rps,
+                  Mps=Mps, Jxyz=Jxyz, Jxx=Jxx, Jyy=Jyy, Jzz=Jzz, uV=uV, iuV=iuV, a_tbl=a_tbl)
+    kAc = np.ascontiguousarray(kAc0 + rng.uniform(-0.05, 0.05, (3, 1)))
+    NL = NLx * NLy * NLz
+    zu = rng.standard_normal((nk, nb, NL)) + 1j * rng.standard_normal((nk, nb, NL))
+    zu = orthonormalise(zu, Hxyz)
+    return sysm, kAc, vloc, zu

@@ -1,0 +1,162 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Tolerances (max |gpu - oracle| / max |oracle|):
+  complex(8) path:  1e-12 for H psi, the Taylor step and every FP64 reduction
+  complex(4) path:  H psi 2e-6, one Taylor step 2e-6 (FP32 orbitals and stencil);
+                    reductions of the complex(4) orbitals 1e-12 against the oracle
+                    run on the same rounded orbitals (they accumulate in FP64)
+"""
+import numpy as np
+import pytest
+
+from _helpers import grid_system, rel
+from oracle import oracle as O
+from salmon_b200 import system as S
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL32_HPSI = 2e-6
+TOL32_STEP = 2e-6
+
+CASES = {
+    "ragged_even_z": lambda: S.small_system(8, 10, 12, nk=3, nb=4, seed=21),
+    "ragged_odd_z": lambda: S.small_system(9, 8, 11, nk=2, nb=3, seed=22),
+    "microbench_20": lambda: S.microbench_system(20, nk_limit=2, Nb=32),
+    "microbench_16": lambda: S.microbench_system(16, nk_limit=1, Nb=32),
+}
+
+
+@pytest.fixture(scope="module", params=sorted(CASES))
+def case(request, cuda_lib):
+    sysm, kAc, vloc, zu = CASES[request.param]()
+    _, zproj = O.update_projector(sysm, kAc)
+    return request.param, sysm, kAc, vloc, zu, zproj
+
+
+def make_gpu(sysm, kAc, vloc, zu, precision="c128"):
+    from salmon_b200.rt import GpuSystem
+    g = GpuSystem(sysm, precision)
+    g.set_state(zu)
+    g.set_vloc(vloc)
+    g.update_projector(kAc)
+    return g
+
+
+def c64_round(z):
+    return z.astype(np.complex64).astype(np.complex128)
+
+
+def test_state_round_trip(case):
+    _, sysm, kAc, vloc, zu, _ = case
+    with make_gpu(sysm, kAc, vloc, zu) as g:
+        np.testing.assert_array_equal(g.get_state(), zu)
+    with make_gpu(sysm, kAc, vloc, zu, "c64") as g:
+        np.testing.assert_array_equal(g.get_state(), c64_round(zu))
+
+
+@pytest.mark.parametrize("precision", ["c128", "c64"])
+def test_hpsi_matches_oracle(case, precision):
+    _, sysm, kAc, vloc, zu, zproj = case
+    tol = TOL64 if precision == "c128" else TOL32_HPSI
+    with make_gpu(sysm, kAc, vloc, zu, precision) as g:
+        for ikl in range(sysm.nk_local):
+            ik = sysm.NK_s + ikl
+            t = zu[ikl, -1]
+            h_ref, tt_ref = O.hpsi(sysm, kAc, vloc, zproj, ik, t, want_tt=True)
+            h = g.hpsi_omp_KB_RT(ik, t)
+            assert rel(h, h_ref) < tol
+            h2, tt = g.hpsi_omp_KB_GS(ik, t)
+            assert rel(h2, h_ref) < tol
+            assert rel(tt, tt_ref) < tol
+
+
+def test_taylor_step_c128(case):
+    _, sysm, kAc, vloc, zu, zproj = case
+    dt = 0.08
+    with make_gpu(sysm, kAc, vloc, zu) as g:
+        g.hamiltonian(dt)
+        z_ref = O.hamiltonian(sysm, kAc, vloc, zproj, dt, zu)
+        assert rel(g.get_state(), z_ref) < TOL64
+        # two more steps at a new k+A(t), as dt_evolve does (update_projector, then hamiltonian)
+        k2 = kAc + np.array([0.0, 0.0, 2e-3])[:, None]
+        _, zp2 = O.update_projector(sysm, k2)
+        g.update_projector(k2)
+        g.hamiltonian(dt)
+        g.hamiltonian(dt)
+        z_ref = O.hamiltonian(sysm, k2, vloc, zp2, dt, O.hamiltonian(sysm, k2, vloc, zp2, dt, z_ref))
+        assert rel(g.get_state(), z_ref) < TOL64
+
+
+def test_taylor_step_c64(case):
+    _, sysm, kAc, vloc, zu, zproj = case
+    dt = 0.08
+    with make_gpu(sysm, kAc, vloc, zu, "c64") as g:
+        g.hamiltonian(dt)
+        z_ref = O.hamiltonian(sysm, kAc, vloc, zproj, dt, c64_round(zu))
+        assert rel(g.get_state(), z_ref) < TOL32_STEP
+
+
+@pytest.mark.parametrize("precision", ["c128", "c64"])
+def test_reductions_fp64(case, precision):
+    _, sysm, kAc, vloc, zu, _ = case
+    z_in = zu if precision == "c128" else c64_round(zu)
+    kcur = kAc + np.array([0.0, 1e-3, 0.0])[:, None]
+    with make_gpu(sysm, kAc, vloc, zu, precision) as g:
+        assert rel(g.psi_rho_RT(), O.psi_rho(sysm, z_in)) < TOL64
+        assert rel(g.current_RT(kcur), O.current(sysm, kcur, z_in)) < TOL64
+        ek, en = g.energy_terms(kcur)
+        ek_ref, en_ref = O.energy_terms(sysm, kcur, z_in)
+        assert abs(ek - ek_ref) < TOL64 * abs(ek_ref)
+        assert abs(en - en_ref) < TOL64 * max(abs(en_ref), 1e-300)
+
+
+def test_hpsi_batch_device_pointers(case):
+    import torch
+    _, sysm, kAc, vloc, zu, zproj = case
+    with make_gpu(sysm, kAc, vloc, zu) as g:
+        nb = min(5, sysm.nk_local * sysm.NBoccmax)
+        src = torch.from_numpy(zu.reshape(-1, sysm.NL)[:nb].copy()).cuda()
+        dst = torch.empty_like(src)
+        torch.cuda.synchronize()
+        g.hpsi_batch(1, nb, src.data_ptr(), dst.data_ptr())
+        g.synchronize()
+        out = dst.cpu().numpy()
+        for o in range(nb):
+            ik = sysm.NK_s + o // sysm.NBoccmax
+            assert rel(out[o], O.hpsi(sysm, kAc, vloc, zproj, ik, zu.reshape(-1, sysm.NL)[o])) < TOL64
+
+
+def test_no_projectors(cuda_lib):
+    """NI = 0: the stencil alone (the reference's stencilperf configuration, Nlma=0)."""
+    sysm = grid_system((10, 12, 8), nk=2, nb=3)
+    sysm.kAc0 = np.array([[0.1, -0.2], [0.05, 0.0], [0.3, 0.1]])
+    rng = np.random.default_rng(0)
+    zu = rng.standard_normal((2, 3, sysm.NL)) + 1j * rng.standard_normal((2, 3, sysm.NL))
+    vloc = rng.uniform(-1, 0, sysm.NL)
+    kAc = sysm.kAc0
+    _, zproj = O.update_projector(sysm, kAc)
+    with make_gpu(sysm, kAc, vloc, zu) as g:
+        g.hamiltonian(0.05)
+        assert rel(g.get_state(), O.hamiltonian(sysm, kAc, vloc, zproj, 0.05, zu)) < TOL64
+
+
+def test_precision_switch_keeps_state(cuda_lib):
+    sysm, kAc, vloc, zu = S.small_system(8, 8, 10, nk=1, nb=2, seed=9)
+    with make_gpu(sysm, kAc, vloc, zu) as g:
+        g.set_precision("c64")
+        np.testing.assert_array_equal(g.get_state(), c64_round(zu))
+        g.set_precision("c128")
+        np.testing.assert_array_equal(g.get_state(), c64_round(zu))
+
+
+def test_errors_are_reported_not_fatal(cuda_lib):
+    from salmon_b200.rt import GpuSystem, SalmonGPUError
+    sysm, kAc, vloc, zu = S.small_system(8, 8, 10, nk=1, nb=2, seed=9)
+    with GpuSystem(sysm) as g:
+        with pytest.raises(SalmonGPUError, match="state, Vloc and projectors"):
+            g.hamiltonian(0.1)
+        g.set_vloc(vloc)
+        g.update_projector(kAc)
+        with pytest.raises(SalmonGPUError, match="ik outside"):
+            g.hpsi_omp_KB_RT(5, zu[0, 0])
