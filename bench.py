@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--only", choices=["c128", "c64"], help="run one precision (profiling)")
+    p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling)")
     return p.parse_args()
 
 
@@ -217,7 +219,7 @@ def main():
         return x
 
     clocks = None
-    for prec in ("c128", "c64"):
+    for prec in ((args.only,) if args.only else ("c128", "c64")):
         S_bytes = 16 if prec == "c128" else 8
         g = GpuSystem(sysm, prec)
         g.set_state(zu)
@@ -253,6 +255,10 @@ def main():
         alg = 2.0 * S_bytes * NL * norb  # algorithmic bytes of one H application over all orbitals
         r.update(t_pass_ms=t_pass, t_last_ms=t_last, t_uvpsi_ms=t_uv, achieved_gbs=alg / (t_pass * 1e-3) / 1e9,
                  step_gbs=10.0 * S_bytes * NL * norb / (r["ms_per_step"] * 1e-3) / 1e9)
+        if args.no_e2e:
+            res[prec] = r
+            g.close()
+            continue
         # end to end through the C ABI with host buffers: k+A(t) and V_loc in, rho and J out, every step
         kA = np.ascontiguousarray(kAc)
         e0.record(stream)
@@ -283,7 +289,9 @@ def main():
             cpu = cpu_baseline(sysm, kAc, vloc, zu, args.cpu_seconds)
         except Exception as exc:  # the CPU baseline is reported, never required
             cpu = {"unavailable": str(exc)}
-    if rank == 0:
+    if rank == 0 and (args.only or args.no_e2e):
+        print(json.dumps({p: {k: v for k, v in r.items() if k != "e2e"} for p, r in res.items()}))
+    elif rank == 0:
         h = res["c64"]
         traffic = NCU_TRAFFIC_BYTES.get(("stencil_pass", "c64", args.grid))
         out = {

@@ -183,6 +183,37 @@ int sgpu_current(sgpu_handle h, const double* kAc, double* jav);
  * (common/total_energy.f90:113-203, stencil/F90/total_energy.f90:25-188). */
 int sgpu_energy_terms(sgpu_handle h, const double* kAc, double* ekin, double* enl);
 
+/* ---- ground state (FP64 in every precision mode) -------------------------- */
+
+/* HOST zu_GS(NL,NB,NK_s:NK_e) -> device (ground-state orbitals, all NB bands). */
+int sgpu_gs_set_state(sgpu_handle h, const double* zu_gs);
+
+/* device -> HOST zu_GS(NL,NB,NK_s:NK_e). */
+int sgpu_gs_get_state(sgpu_handle h, double* zu_gs);
+
+/* Gram-Schmidt of the ground-state bands of every k-point, band by band
+ * against the lower bands.  Replaces Gram_Schmidt_ompk
+ * (GS/Gram_Schmidt.f90:32-55). */
+int sgpu_gram_schmidt(sgpu_handle h);
+
+/* ncg band-by-band CG iterations on the ground-state orbitals with the
+ * Hamiltonian of the last sgpu_update_projector / sgpu_set_vloc.  esp_var
+ * (NB,NK_s:NK_e) HOST receives the residual norms times occ before the
+ * allreduce (may be NULL); iters (NB,NK_s:NK_e) HOST the CG iterations run per
+ * band (may be NULL).  Replaces CG_ompk (GS/CG.f90:34-139). */
+int sgpu_cg(sgpu_handle h, int ncg, double* esp_var, int* iters);
+
+/* Subspace diagonalisation: H_sub(NB,NB) per k-point, its Hermitian
+ * eigen-decomposition (ascending eigenvalues) and the rotation of the bands.
+ * esp (NB,NK_s:NK_e) HOST receives the eigenvalues (may be NULL).  Replaces
+ * diag_omp (GS/diag.f90:22-173); the eigen-solver is a cyclic Jacobi on the GPU
+ * in place of LAPACK zheev. */
+int sgpu_subspace_diag(sgpu_handle h, double* esp);
+
+/* zu_t(:,1:NBoccmax,:) = zu_GS(:,1:NBoccmax,:) on the device (the start of the
+ * real-time run), converted to the handle's precision. */
+int sgpu_gs_to_rt(sgpu_handle h);
+
 /* ---- instrumentation ----------------------------------------------------- */
 /* Kernels that sgpu_time_kernel can time. */
 enum {

@@ -35,6 +35,12 @@ ABI = {
     "sgpu_current": (C.c_int, [_vp, _vp, _vp]),
     "sgpu_energy_terms": (C.c_int, [_vp, _vp, _dp, _dp]),
     "sgpu_time_kernel": (C.c_int, [_vp, _ip, _ip, _dp]),
+    "sgpu_gs_set_state": (C.c_int, [_vp, _vp]),
+    "sgpu_gs_get_state": (C.c_int, [_vp, _vp]),
+    "sgpu_gram_schmidt": (C.c_int, [_vp]),
+    "sgpu_cg": (C.c_int, [_vp, _ip, _vp, _vp]),
+    "sgpu_subspace_diag": (C.c_int, [_vp, _vp]),
+    "sgpu_gs_to_rt": (C.c_int, [_vp]),
 }
 
 KERNELS = {"stencil_pass": 0, "taylor_last": 1, "uvpsi": 2, "psi_rho": 3}

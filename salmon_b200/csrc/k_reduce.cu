@@ -341,7 +341,7 @@ cudaError_t launch_energy(System& s, double* e_dev) {
   if (err != cudaSuccess) return err;
   // U = Hxyz * sum conj(zproj) psi = Hxyz * sum uV ekr psi  (total_energy.f90:191-197), FP64 projectors
   if (s.Nlma) {
-    err = launch_uvpsi(s, s.zu, 0, s.norb, false);
+    err = launch_uvpsi(s, s.zu, 0, s.norb, s.NBocc, false);
     if (err != cudaSuccess) return err;
   }
   k_energy_final<<<1, 256, 0, s.stream>>>(orb, s.U, s.occ_o, s.kAc_d, s.iuV_d, s.norb, s.NBocc, s.Nlma, s.Hxyz, e_dev);

@@ -128,6 +128,9 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
     s->lap[0][n] = d->lapx[n]; s->lap[1][n] = d->lapy[n]; s->lap[2][n] = d->lapz[n];
     s->nab[0][n] = d->nabx[n]; s->nab[1][n] = d->naby[n]; s->nab[2][n] = d->nabz[n];
   }
+  s->cubic = true;
+  for (int n = 0; n < 5; ++n)
+    s->cubic = s->cubic && d->lapx[n] == d->lapy[n] && d->lapx[n] == d->lapz[n] && (n == 0 || (d->nabx[n] == d->naby[n] && d->nabx[n] == d->nabz[n]));
   s->NI = d->Nlma > 0 ? d->NI : 0;
   s->Nps = d->Nlma > 0 ? d->Nps : 0;
   s->Nlma = d->Nlma;
@@ -189,6 +192,37 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
     }
   }
   s->ninv = (int)ent.size();
+  // sphere points by x-plane with their <= 4 (ilma, j) entries, and the map from
+  // packed projector points to sphere points
+  std::vector<int> sp_off(s->NLx + 1, 0), q_of(s->NL, -1), qmap(std::max(1, s->NPI), 0);
+  std::vector<int4> rec;
+  {
+    if (s->Nps >= 65536 || s->Nlma >= 32768)
+      return bail(fail(SGPU_ERR_UNSUPPORTED, "sgpu_create: Nps must be < 65536 and Nlma < 32768"));
+    const int NYZ = s->NLy * s->NLz;
+    int nsp = 0;
+    for (int x = 0; x < s->NLx; ++x) {
+      sp_off[x] = nsp;
+      for (int i = x * NYZ; i < (x + 1) * NYZ; ++i) {
+        const int c = cnt[i + 1] - cnt[i];
+        if (c == 0) continue;
+        if (c > 4)
+          return bail(fail(SGPU_ERR_UNSUPPORTED,
+                           "sgpu_create: a grid point lies in more than 4 projector spheres (entries per point > 4)"));
+        int e[4] = {0, 0, 0, 0};
+        for (int k = 0; k < c; ++k) {
+          const int2 en = ent[cnt[i] + k];  // {ilma*Nps + j, ilma}
+          e[k] = (en.y << 16) | (en.x - en.y * s->Nps);
+        }
+        rec.push_back(make_int4(i - x * NYZ, c, e[0], e[1]));
+        rec.push_back(make_int4(e[2], e[3], 0, 0));
+        q_of[i] = nsp++;
+      }
+    }
+    sp_off[s->NLx] = nsp;
+    s->nsp = nsp;
+    for (int p = 0; p < s->NPI; ++p) qmap[p] = q_of[idx_proj[p]];
+  }
   std::vector<double> uv((size_t)s->Nlma * s->Nps);
   if (s->Nlma) std::memcpy(uv.data(), d->uV, uv.size() * sizeof(double));
 
@@ -210,8 +244,9 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
   UP(s->iuV_d, iuv);
   UP(s->lma_atom, lma_atom);
   UP(s->uV_d, uv);
-  UP(s->inv_off, cnt);
-  UP(s->inv_ent, ent);
+  UP(s->sp_off, sp_off);
+  UP(s->rec, rec);
+  UP(s->qmap, qmap);
   UP(s->occ_o, occo);
 #undef UP
   const size_t nz = (size_t)s->nkl * s->Nlma * s->Nps;
@@ -222,6 +257,9 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
   if ((e = cudaMemsetAsync(s->zproj32, 0, std::max<size_t>(nz, 1) * sizeof(float2), s->stream)) != cudaSuccess)
     return bail(cuda_fail(e, "memset zproj32"));
   if ((e = dalloc(&s->U, (size_t)s->norb * std::max(1, s->Nlma))) != cudaSuccess) return bail(cuda_fail(e, "alloc U"));
+  s->U_rows = (size_t)s->norb;
+  if ((e = cudaMalloc(&s->Sbuf, (size_t)s->norb * std::max(1, s->nsp) * sizeof(double2))) != cudaSuccess)
+    return bail(cuda_fail(e, "alloc S"));
   if ((e = dalloc(&s->Uw, (size_t)s->norb * std::max(1, s->Nlma) * 4)) != cudaSuccess)
     return bail(cuda_fail(e, "alloc Uw"));
   if ((e = dalloc(&s->kAc_d, 3 * (size_t)s->nkl)) != cudaSuccess) return bail(cuda_fail(e, "alloc kAc"));
@@ -251,9 +289,13 @@ int sgpu_destroy(sgpu_handle h) {
   if (s->stream) cudaStreamSynchronize(s->stream);
   free_state_buffers(s);
   void* bufs[] = {s->vloc64, s->vloc32, s->occ_o, s->kAc_d, s->idx_proj, s->atom_off, s->rpos, s->items,
-                  s->lma_list, s->iuV_d, s->lma_atom, s->uV_d, s->zproj64, s->zproj32, s->inv_off, s->inv_ent,
+                  s->lma_list, s->iuV_d, s->lma_atom, s->uV_d, s->zproj64, s->zproj32, s->sp_off, s->rec, s->qmap, s->Sbuf,
                   s->U, s->Uw, s->red, s->stage};
   for (void* p : bufs) cudaFree(p);
+  void* gbufs[] = {s->gs_zu, s->gs_aux, s->gs_W, s->gs_st, s->gs_part, s->gs_A, s->gs_V, s->gs_w, s->gs_sweeps,
+                   s->occ_gs, s->gs_out};
+  for (void* p : gbufs) cudaFree(p);
+  if (s->gs_h) cudaFreeHost(s->gs_h);
   if (s->red_h) cudaFreeHost(s->red_h);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete h;
@@ -285,6 +327,7 @@ int sgpu_set_state(sgpu_handle h, const double* zu) {
   }
   CK(cudaStreamSynchronize(s->stream));
   s->have_state = true;
+  s->S_valid = false;
   return 0;
 }
 
@@ -317,6 +360,7 @@ int sgpu_set_precision(sgpu_handle h, int precision) {
   for (auto& t : s->tw) { cudaFree(t); t = nullptr; }
   s->zu = nullptr;
   s->prec = precision;
+  s->S_valid = false;
   s->elem = precision == SGPU_PREC_C64 ? sizeof(float2) : sizeof(double2);
   CK(cudaMalloc(&s->zu, n * s->elem));
   if (s->have_state) {
@@ -368,21 +412,28 @@ int sgpu_hamiltonian(sgpu_handle h, double dt, int flag_current) {
     io.zfac[i - 1][0] = (pr * 0.0 - pi * (-dt)) / i;
     io.zfac[i - 1][1] = (pr * (-dt) + pi * 0.0) / i;
   }
+  // Each pass exports its output at the sphere points (S); the next pass's
+  // projections read S instead of gathering from the full orbitals.
   const void* ins[4] = {s->zu, s->tw[0], s->tw[1], s->tw[2]};
   for (int n = 0; n < 4; ++n) {
-    CK(sgpu::launch_uvpsi(*s, ins[n], 0, s->norb, true));
+    if (n == 0 && !s->S_valid)
+      CK(sgpu::launch_uvpsi(*s, ins[0], 0, s->norb, s->NBocc, true));
+    else
+      CK(sgpu::launch_uvpsi_from_S(*s, s->Sbuf, 0, s->norb, s->NBocc, true));
     io.in = ins[n];
+    io.S = s->nsp > 0 ? s->Sbuf : nullptr;
     if (n < 3) {
       io.out = s->tw[n];
-      CK(sgpu::launch_hpsi_pass(*s, 0, io, 0, s->norb));
+      CK(sgpu::launch_hpsi_pass(*s, 0, io, 0, s->norb, s->NBocc));
     } else {
       io.out = nullptr;
       io.t1 = s->tw[0];
       io.t2 = s->tw[1];
       io.zu = s->zu;
-      CK(sgpu::launch_hpsi_pass(*s, 2, io, 0, s->norb));
+      CK(sgpu::launch_hpsi_pass(*s, 2, io, 0, s->norb, s->NBocc));
     }
   }
+  s->S_valid = s->nsp > 0;
   return 0;
 }
 
@@ -405,14 +456,14 @@ int sgpu_hpsi(sgpu_handle h, int ik, const double* tpsi, double* htpsi, double* 
     float2* tt32 = (float2*)s->tw[2];
     CK(sgpu::launch_c128_to_c64(in128, in32, NL, s->stream));
     io.in = in32; io.out = out32; io.tt = tt32;
-    CK(sgpu::launch_uvpsi(*s, in32, ob, 1, true));
-    CK(sgpu::launch_hpsi_pass(*s, ttpsi ? 1 : 0, io, ob, 1));
+    CK(sgpu::launch_uvpsi(*s, in32, ob, 1, s->NBocc, true));
+    CK(sgpu::launch_hpsi_pass(*s, ttpsi ? 1 : 0, io, ob, 1, s->NBocc));
     CK(sgpu::launch_c64_to_c128(out32, out128, NL, s->stream));
     if (ttpsi) CK(sgpu::launch_c64_to_c128(tt32, tt128, NL, s->stream));
   } else {
     io.in = in128; io.out = out128; io.tt = tt128;
-    CK(sgpu::launch_uvpsi(*s, in128, ob, 1, true));
-    CK(sgpu::launch_hpsi_pass(*s, ttpsi ? 1 : 0, io, ob, 1));
+    CK(sgpu::launch_uvpsi(*s, in128, ob, 1, s->NBocc, true));
+    CK(sgpu::launch_hpsi_pass(*s, ttpsi ? 1 : 0, io, ob, 1, s->NBocc));
   }
   CK(cudaMemcpyAsync(htpsi, out128, NL * sizeof(double2), cudaMemcpyDeviceToHost, s->stream));
   if (ttpsi) CK(cudaMemcpyAsync(ttpsi, tt128, NL * sizeof(double2), cudaMemcpyDeviceToHost, s->stream));
@@ -425,12 +476,14 @@ int sgpu_hpsi_batch(sgpu_handle h, int ikb_s, int ikb_e, const void* tpsi, void*
   System* s = h;
   if (ikb_s < 1 || ikb_e < ikb_s || ikb_e > s->norb) return fail(SGPU_ERR_ARG, "sgpu_hpsi_batch: bad ikb range");
   if (!s->have_vloc || !s->have_proj) return fail(SGPU_ERR_STATE, "sgpu_hpsi_batch: Vloc and projectors must be set first");
+  if (((uintptr_t)tpsi | (uintptr_t)htpsi) % 16 != 0)
+    return fail(SGPU_ERR_ARG, "sgpu_hpsi_batch: tpsi and htpsi must be 16-byte aligned");
   const int nb = ikb_e - ikb_s + 1;
   sgpu::PassIO io;
   io.in = tpsi;
   io.out = htpsi;
-  CK(sgpu::launch_uvpsi(*s, tpsi, ikb_s - 1, nb, true));
-  CK(sgpu::launch_hpsi_pass(*s, 0, io, ikb_s - 1, nb));
+  CK(sgpu::launch_uvpsi(*s, tpsi, ikb_s - 1, nb, s->NBocc, true));
+  CK(sgpu::launch_hpsi_pass(*s, 0, io, ikb_s - 1, nb, s->NBocc));
   return 0;
 }
 
@@ -487,20 +540,21 @@ int sgpu_time_kernel(sgpu_handle h, int kernel, int reps, double* ms_per_launch)
   CK(cudaEventCreate(&e1));
   auto launch = [&]() -> cudaError_t {
     switch (kernel) {
-      case SGPU_KERNEL_STENCIL_PASS:
-        io.in = s->zu; io.out = s->tw[0];
-        return sgpu::launch_hpsi_pass(*s, 0, io, 0, s->norb);
+      case SGPU_KERNEL_STENCIL_PASS:  // as in the Taylor step: with the sphere-value export
+        io.in = s->zu; io.out = s->tw[0]; io.S = s->nsp > 0 ? s->Sbuf : nullptr;
+        return sgpu::launch_hpsi_pass(*s, 0, io, 0, s->norb, s->NBocc);
       case SGPU_KERNEL_TAYLOR_LAST:  // reads tw[2], tw[0], tw[1] and updates tw[2] in place (zu untouched)
-        io.in = s->tw[0]; io.t1 = s->tw[1]; io.t2 = s->tw[1]; io.zu = s->tw[2];
-        return sgpu::launch_hpsi_pass(*s, 2, io, 0, s->norb);
-      case SGPU_KERNEL_UVPSI:
-        return sgpu::launch_uvpsi(*s, s->zu, 0, s->norb, true);
+        io.in = s->tw[0]; io.t1 = s->tw[1]; io.t2 = s->tw[1]; io.zu = s->tw[2]; io.S = s->nsp > 0 ? s->Sbuf : nullptr;
+        return sgpu::launch_hpsi_pass(*s, 2, io, 0, s->norb, s->NBocc);
+      case SGPU_KERNEL_UVPSI:  // projections from the exported sphere values (passes 2-4 of a step)
+        return sgpu::launch_uvpsi_from_S(*s, s->Sbuf, 0, s->norb, s->NBocc, true);
       case SGPU_KERNEL_PSI_RHO:
         return sgpu::launch_psi_rho(*s, (double*)s->stage);
       default:
         return cudaErrorInvalidValue;
     }
   };
+  s->S_valid = false;           // the timed launches overwrite S with workspace values
   cudaError_t err = launch();  // warm-up (and argument check)
   if (err == cudaSuccess) err = cudaEventRecord(e0, s->stream);
   for (int r = 0; r < reps && err == cudaSuccess; ++r) err = launch();
@@ -512,6 +566,173 @@ int sgpu_time_kernel(sgpu_handle h, int kernel, int reps, double* ms_per_launch)
   cudaEventDestroy(e1);
   if (err != cudaSuccess) return cuda_fail(err, "sgpu_time_kernel");
   *ms_per_launch = ms / reps;
+  return 0;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------ ground state --
+namespace {
+
+int gs_alloc(System* s) {
+  if (s->gs_zu) return 0;
+  const size_t nbl = (size_t)s->nkl * s->NB * s->NL;
+  const int nt = (s->NB + 15) / 16;
+  // split K so that the subspace GEMM has at least ~4 CTAs per SM
+  s->gs_nsplit = std::max(1, std::min(64, (4 * 148 + s->nkl * nt * nt - 1) / std::max(1, s->nkl * nt * nt)));
+  CK(cudaMalloc(&s->gs_zu, nbl * sizeof(double2)));
+  CK(cudaMalloc(&s->gs_aux, nbl * sizeof(double2)));
+  CK(cudaMalloc(&s->gs_W, (size_t)sgpu::cg_work_vectors() * s->nkl * s->NL * sizeof(double2)));
+  CK(cudaMalloc(&s->gs_st, s->nkl * sgpu::cg_state_bytes()));
+  CK(cudaMalloc(&s->gs_part, (size_t)s->gs_nsplit * s->nkl * s->NB * s->NB * sizeof(double2)));
+  CK(cudaMalloc(&s->gs_A, (size_t)s->nkl * s->NB * s->NB * sizeof(double2)));
+  CK(cudaMalloc(&s->gs_V, (size_t)s->nkl * s->NB * s->NB * sizeof(double2)));
+  CK(cudaMalloc(&s->gs_w, (size_t)s->nkl * s->NB * sizeof(double)));
+  CK(cudaMalloc(&s->gs_sweeps, (size_t)s->nkl * sizeof(int)));
+  CK(cudaMalloc(&s->gs_out, (size_t)s->nkl * s->NB * sizeof(double)));
+  CK(cudaMallocHost((void**)&s->gs_h, (size_t)s->nkl * s->NB * sizeof(double)));
+  std::vector<double> occ((size_t)s->nkl * s->NB);
+  for (int kl = 0; kl < s->nkl; ++kl)
+    for (int b = 0; b < s->NB; ++b) occ[(size_t)kl * s->NB + b] = s->occ_h[(size_t)(s->NK_s - 1 + kl) * s->NB + b];
+  CK(cudaMalloc(&s->occ_gs, occ.size() * sizeof(double)));
+  CK(cudaMemcpyAsync(s->occ_gs, occ.data(), occ.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  const size_t rows = std::max((size_t)s->norb, (size_t)s->nkl * s->NB);
+  if (rows > s->U_rows) {
+    CK(cudaStreamSynchronize(s->stream));
+    cudaFree(s->U);
+    s->U = nullptr;
+    CK(cudaMalloc(&s->U, rows * std::max(1, s->Nlma) * sizeof(double2)));
+    s->U_rows = rows;
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+// FP64 H applied to a batch of nb vectors of the k-points o/nbk (mode 0 or 1)
+int gs_hpsi(System* s, const double2* in, double2* out, double2* tt, int nb, int nbk) {
+  sgpu::PassIO io;
+  io.in = in;
+  io.out = out;
+  io.tt = tt;
+  CK(sgpu::launch_uvpsi(*s, in, 0, nb, nbk, true, SGPU_PREC_C128));
+  CK(sgpu::launch_hpsi_pass(*s, tt ? 1 : 0, io, 0, nb, nbk, SGPU_PREC_C128));
+  return 0;
+}
+
+int gs_ready(System* s, const char* who) {
+  if (!s->have_gs) return fail(SGPU_ERR_STATE, std::string(who) + ": no ground-state orbitals loaded");
+  if (!s->have_vloc || !s->have_proj) return fail(SGPU_ERR_STATE, std::string(who) + ": Vloc and projectors must be set first");
+  return 0;
+}
+
+int gs_copy_out(System* s, const double* dev, double* host) {
+  if (!host) return 0;
+  const size_t n = (size_t)s->nkl * s->NB;
+  CK(cudaMemcpyAsync(s->gs_h, dev, n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  std::memcpy(host, s->gs_h, n * sizeof(double));
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sgpu_gs_set_state(sgpu_handle h, const double* zu_gs) {
+  if (!valid(h) || !zu_gs) return fail(SGPU_ERR_ARG, "sgpu_gs_set_state: null argument");
+  System* s = h;
+  int rc = gs_alloc(s);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(s->gs_zu, zu_gs, (size_t)s->nkl * s->NB * s->NL * sizeof(double2), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  s->have_gs = true;
+  return 0;
+}
+
+int sgpu_gs_get_state(sgpu_handle h, double* zu_gs) {
+  if (!valid(h) || !zu_gs) return fail(SGPU_ERR_ARG, "sgpu_gs_get_state: null argument");
+  System* s = h;
+  if (!s->have_gs) return fail(SGPU_ERR_STATE, "sgpu_gs_get_state: no ground-state orbitals loaded");
+  CK(cudaMemcpyAsync(zu_gs, s->gs_zu, (size_t)s->nkl * s->NB * s->NL * sizeof(double2), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int sgpu_gram_schmidt(sgpu_handle h) {
+  if (!valid(h)) return fail(SGPU_ERR_ARG, "null handle");
+  System* s = h;
+  if (!s->have_gs) return fail(SGPU_ERR_STATE, "sgpu_gram_schmidt: no ground-state orbitals loaded");
+  CK(sgpu::launch_gram_schmidt(*s, s->gs_zu));
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int sgpu_cg(sgpu_handle h, int ncg, double* esp_var, int* iters) {
+  if (!valid(h) || ncg < 1) return fail(SGPU_ERR_ARG, "sgpu_cg: bad argument");
+  System* s = h;
+  int rc = gs_ready(s, "sgpu_cg");
+  if (rc) return rc;
+  const size_t NL = s->NL, nk = s->nkl;
+  double2* W = s->gs_W;
+  auto vec = [&](int which) { return W + (size_t)which * nk * NL; };
+  std::vector<int> it_all(iters ? (size_t)s->nkl * s->NB : 0);
+  std::vector<char> st_h(s->nkl * sgpu::cg_state_bytes());
+  for (int ib = 0; ib < s->NB; ++ib) {
+    CK(sgpu::launch_cg_begin(*s, s->gs_zu, W, s->gs_st, ib));
+    if ((rc = gs_hpsi(s, vec(0), vec(1), vec(2), s->nkl, 1))) return rc;   // xk -> hxk, txk
+    CK(sgpu::launch_cg_dot0(*s, W, s->gs_st));
+    for (int iter = 1; iter <= ncg; ++iter) {
+      CK(sgpu::launch_cg_pre(*s, s->gs_zu, W, s->gs_st, ib, iter));
+      if ((rc = gs_hpsi(s, vec(5), vec(6), vec(7), s->nkl, 1))) return rc; // pko -> htpsi, ttpsi
+      CK(sgpu::launch_cg_post(*s, W, s->gs_st, iter));
+    }
+    CK(sgpu::launch_cg_end(*s, s->gs_zu, W, ib));
+    if ((rc = gs_hpsi(s, vec(0), vec(6), nullptr, s->nkl, 1))) return rc;  // H u_ib
+    CK(sgpu::launch_cg_resid(*s, W, s->occ_gs, s->gs_out, ib));
+    if (iters) {
+      CK(cudaMemcpyAsync(st_h.data(), s->gs_st, st_h.size(), cudaMemcpyDeviceToHost, s->stream));
+      CK(cudaStreamSynchronize(s->stream));
+      for (int k = 0; k < s->nkl; ++k) {
+        int v;
+        std::memcpy(&v, st_h.data() + k * sgpu::cg_state_bytes() + 2 * sizeof(double) + sizeof(int), sizeof(int));
+        it_all[(size_t)k * s->NB + ib] = v;
+      }
+    }
+  }
+  if ((rc = gs_copy_out(s, s->gs_out, esp_var))) return rc;
+  if (iters) std::memcpy(iters, it_all.data(), it_all.size() * sizeof(int));
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int sgpu_subspace_diag(sgpu_handle h, double* esp) {
+  if (!valid(h)) return fail(SGPU_ERR_ARG, "null handle");
+  System* s = h;
+  int rc = gs_ready(s, "sgpu_subspace_diag");
+  if (rc) return rc;
+  if ((rc = gs_hpsi(s, s->gs_zu, s->gs_aux, nullptr, s->nkl * s->NB, s->NB))) return rc;
+  CK(sgpu::launch_subspace_h(*s, s->gs_zu, s->gs_aux, s->gs_part, s->gs_nsplit, s->gs_A));
+  CK(sgpu::launch_jacobi(*s, s->gs_A, s->gs_V, 30, s->gs_w, s->gs_sweeps));
+  CK(sgpu::launch_rotate(*s, s->gs_zu, s->gs_A, s->gs_aux));
+  std::swap(s->gs_zu, s->gs_aux);
+  return gs_copy_out(s, s->gs_w, esp) ? SGPU_ERR_CUDA : (cudaStreamSynchronize(s->stream) == cudaSuccess ? 0 : cuda_fail(cudaGetLastError(), "sgpu_subspace_diag"));
+}
+
+int sgpu_gs_to_rt(sgpu_handle h) {
+  if (!valid(h)) return fail(SGPU_ERR_ARG, "null handle");
+  System* s = h;
+  if (!s->have_gs) return fail(SGPU_ERR_STATE, "sgpu_gs_to_rt: no ground-state orbitals loaded");
+  const size_t run = (size_t)s->NBocc * s->NL;
+  for (int k = 0; k < s->nkl; ++k) {
+    const double2* src = s->gs_zu + (size_t)k * s->NB * s->NL;
+    if (s->prec == SGPU_PREC_C128)
+      CK(cudaMemcpyAsync((double2*)s->zu + (size_t)k * run, src, run * sizeof(double2), cudaMemcpyDeviceToDevice, s->stream));
+    else
+      CK(sgpu::launch_c128_to_c64(src, (float2*)s->zu + (size_t)k * run, run, s->stream));
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  s->have_state = true;
+  s->S_valid = false;
   return 0;
 }
 

@@ -39,6 +39,28 @@ template <typename R> __device__ __forceinline__ C2<R> from_d2(double2 a);
 template <> __device__ __forceinline__ float2 from_d2<float>(double2 a) { return make_float2((float)a.x, (float)a.y); }
 template <> __device__ __forceinline__ double2 from_d2<double>(double2 a) { return a; }
 
+// Sum of NV doubles over the CTA; the result is valid in every thread.
+// sh must hold 32*NV doubles; the call contains __syncthreads().
+template <int NV>
+__device__ __forceinline__ void block_allsum(double (&v)[NV], double* sh) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int k = 0; k < NV; ++k)
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], off);
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) sh[warp * NV + k] = v[k];
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    double t = 0.0;
+    for (int w = 0; w < nw; ++w) t += sh[w * NV + k];  // fixed order: deterministic
+    v[k] = t;
+  }
+}
+
 // ------------------------------------------------------------ the system --
 // Per-handle state: sizes, constants and device buffers.
 struct System {
@@ -77,8 +99,18 @@ struct System {
   double* uV_d = nullptr;          // [Nlma][Nps]
   double2* zproj64 = nullptr;      // [nkl][Nlma][Nps]
   float2* zproj32 = nullptr;       // [nkl][Nlma][Nps]   (C64 mode)
-  int* inv_off = nullptr;          // [NL+1] CSR of (ilma,j) pairs touching each grid point
-  int2* inv_ent = nullptr;         // [ninv] {ilma*Nps + j, ilma}
+  // Kleinman-Bylander sphere points sorted by grid index: plane x holds points
+  // sp_off[x] .. sp_off[x+1]-1; point q has the record rec[2q..2q+1] =
+  // {in-plane position, entry count (<= 4), e0, e1}, {e2, e3, 0, 0} with
+  // e = ilma<<16 | j (zproj(j,ilma)).  qmap[p] is the sphere-point index of
+  // packed projector point p (the gather index into a sphere-value array S).
+  int* sp_off = nullptr;           // [NLx+1]
+  int4* rec = nullptr;             // [2*nsp]
+  int* qmap = nullptr;             // [NPI]
+  int nsp = 0;
+  void* Sbuf = nullptr;            // [norb][nsp] orbital values at the sphere points
+  bool S_valid = false;            // Sbuf holds the sphere values of the resident zu
+  bool cubic = false;               // lapx==lapy==lapz and nabx==naby==nabz (packed FP32 pass)
   double2* U = nullptr;            // [norb][Nlma] projections <uV e^{ikr}|psi> (scaled)
   double2* Uw = nullptr;           // [norb][Nlma][4] weighted projections for the current
 
@@ -92,16 +124,37 @@ struct System {
   double2* stage = nullptr;        // [stage_elems] complex(8)
   size_t stage_elems = 0;
 
+  // ground state (allocated on first use): zu_GS(NL,NB,NK_s:NK_e) and work space
+  double2* gs_zu = nullptr;        // [nkl][NB][NL]
+  double2* gs_aux = nullptr;       // [nkl][NB][NL]  H zu_GS, rotation output
+  double2* gs_W = nullptr;         // [8][nkl][NL]   CG work vectors
+  void* gs_st = nullptr;           // [nkl] CG state
+  double2* gs_part = nullptr;      // [nsplit][nkl][NB][NB]
+  double2* gs_A = nullptr;         // [nkl][NB][NB]
+  double2* gs_V = nullptr;         // [nkl][NB][NB]
+  double* gs_w = nullptr;          // [nkl][NB]
+  int* gs_sweeps = nullptr;        // [nkl]
+  double* occ_gs = nullptr;        // [nkl][NB]
+  double* gs_out = nullptr;        // [nkl][NB] device results
+  double* gs_h = nullptr;          // pinned host staging [nkl][NB]
+  int gs_nsplit = 0;
+  bool have_gs = false;
+  size_t U_rows = 0;               // orbitals U can hold
+
   // tuning
   int nslab = 1;                   // x-slabs per orbital in the stencil pass
 };
 
 // ------------------------------------------------------------ kernel API --
-// All launches go to s.stream.  Orbitals of a batch are resident indices
-// [o_beg, o_beg+nb); k-point of resident orbital o is o / NBocc.
+// All launches go to s.stream.  A batch is nb orbitals in[0..nb) laid out like
+// zu; orbital b of the batch belongs to local k-point (o_beg + b) / nbk
+// (nbk = NBoccmax for the resident orbitals, NB for ground-state arrays, 1 for
+// one work vector per k-point).
 
 // U[b][ilma] = Hxyz * (scale_iuv ? iuV : 1) * sum_j conj(zproj(j,ilma,k)) in_b(J_a(j))
-cudaError_t launch_uvpsi(const System& s, const void* in, int o_beg, int nb, bool scale_iuv);
+cudaError_t launch_uvpsi(const System& s, const void* in, int o_beg, int nb, int nbk, bool scale_iuv, int prec = -1);
+// the same projections from sphere values S[b][nsp] exported by a pass
+cudaError_t launch_uvpsi_from_S(const System& s, const void* S, int o_beg, int nb, int nbk, bool scale_iuv);
 
 // One H application: out = H in  (mode 0), with ttpsi (mode 1), or the last
 // Taylor pass (mode 2): zu = zu + z1 t1 + z2 t2 + z3 in + z4 H in.  U must hold
@@ -113,9 +166,13 @@ struct PassIO {
   const void* t1 = nullptr;
   const void* t2 = nullptr;
   void* zu = nullptr;
+  void* S = nullptr;               // export of the output at the sphere points ([nb][nsp]) or null
   double zfac[4][2] = {};
 };
-cudaError_t launch_hpsi_pass(const System& s, int mode, const PassIO& io, int o_beg, int nb);
+// prec = -1 uses the handle's precision; SGPU_PREC_C128 forces FP64 (ground state).
+cudaError_t launch_hpsi_pass(const System& s, int mode, const PassIO& io, int o_beg, int nb, int nbk, int prec = -1);
+// threads per CTA of the pass kernel for an NLy x NLz plane
+int pass_block_threads(int NLy, int NLz);
 
 // zproj(j,ilma,k) = conj(exp(i kAc.r)) uV(j,ilma)  for the local k-points.
 cudaError_t launch_update_projector(const System& s);
@@ -131,5 +188,20 @@ cudaError_t launch_psi_rho(System& s, double* rho_dev);
 cudaError_t launch_current(System& s, double* jav_dev);
 // per-orbital kinetic and nonlocal energies summed (device, 2 doubles)
 cudaError_t launch_energy(System& s, double* e_dev);
+
+// ground state (k_gs.cu)
+cudaError_t launch_gram_schmidt(const System& s, double2* zu);
+cudaError_t launch_cg_begin(const System& s, double2* zu, double2* W, void* st, int ib);
+cudaError_t launch_cg_dot0(const System& s, double2* W, void* st);
+cudaError_t launch_cg_pre(const System& s, const double2* zu, double2* W, void* st, int ib, int iter);
+cudaError_t launch_cg_post(const System& s, double2* W, void* st, int iter);
+cudaError_t launch_cg_end(const System& s, double2* zu, double2* W, int ib);
+cudaError_t launch_cg_resid(const System& s, double2* W, const double* occ_gs, double* esp_var, int ib);
+size_t cg_state_bytes();
+int cg_work_vectors();
+cudaError_t launch_subspace_h(const System& s, const double2* U, const double2* HU, double2* part, int nsplit,
+                              double2* za);
+cudaError_t launch_jacobi(const System& s, double2* A, double2* V, int max_sweeps, double* w, int* sweeps);
+cudaError_t launch_rotate(const System& s, const double2* in, const double2* Z, double2* out);
 
 }  // namespace sgpu

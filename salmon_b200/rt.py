@@ -128,6 +128,42 @@ class GpuSystem:
         call("sgpu_time_kernel", self._h, _lib.KERNELS[kernel], reps, C.byref(ms))
         return ms.value
 
+    # ---- ground state (FP64)
+    def gs_set_state(self, zu_gs):
+        s = self.sysm
+        z = np.ascontiguousarray(zu_gs, dtype=np.complex128)
+        if z.shape != (s.nk_local, s.NB, s.NL):
+            raise ValueError(f"zu_GS must have shape {(s.nk_local, s.NB, s.NL)}")
+        call("sgpu_gs_set_state", self._h, _vp(z))
+
+    def gs_get_state(self):
+        s = self.sysm
+        z = np.empty((s.nk_local, s.NB, s.NL), np.complex128)
+        call("sgpu_gs_get_state", self._h, _vp(z))
+        return z
+
+    def gram_schmidt(self):
+        """Gram_Schmidt_ompk (GS/Gram_Schmidt.f90:32-55) on the device ground-state orbitals."""
+        call("sgpu_gram_schmidt", self._h)
+
+    def cg(self, ncg: int):
+        """CG_ompk (GS/CG.f90:34-139); returns (esp_var (nkl,NB), iterations (nkl,NB))."""
+        s = self.sysm
+        esp = np.empty((s.nk_local, s.NB))
+        its = np.empty((s.nk_local, s.NB), np.int32)
+        call("sgpu_cg", self._h, int(ncg), _vp(esp), _vp(its))
+        return esp, its
+
+    def subspace_diag(self):
+        """diag_omp (GS/diag.f90:22-173); returns the eigenvalues esp (nkl,NB)."""
+        s = self.sysm
+        esp = np.empty((s.nk_local, s.NB))
+        call("sgpu_subspace_diag", self._h, _vp(esp))
+        return esp
+
+    def gs_to_rt(self):
+        call("sgpu_gs_to_rt", self._h)
+
     # ---- reductions
     def psi_rho_RT(self):
         rho = np.empty(self.sysm.NL)
