@@ -214,13 +214,25 @@ int sgpu_subspace_diag(sgpu_handle h, double* esp);
  * real-time run), converted to the handle's precision. */
 int sgpu_gs_to_rt(sgpu_handle h);
 
+/* ---- tuning --------------------------------------------------------------- */
+enum {
+  SGPU_PARAM_NSLAB = 0   /* CTAs per orbital along x in the stencil pass (1..NLx) */
+};
+
+/* Sets / reads a launch parameter of the handle (the autotuner's knobs).  No
+ * reference counterpart; the nearest is auto_blocking
+ * (modules/opt_variables.f90:340-353), which picks cache blocking sizes. */
+int sgpu_set_param(sgpu_handle h, int param, int value);
+int sgpu_get_param(sgpu_handle h, int param, int* value);
+
 /* ---- instrumentation ----------------------------------------------------- */
 /* Kernels that sgpu_time_kernel can time. */
 enum {
   SGPU_KERNEL_STENCIL_PASS = 0, /* one H application of every resident orbital (zu -> workspace)     */
   SGPU_KERNEL_TAYLOR_LAST = 1,  /* the fused last Taylor pass (H application + update), on workspace */
   SGPU_KERNEL_UVPSI = 2,        /* the Kleinman-Bylander projections of every resident orbital       */
-  SGPU_KERNEL_PSI_RHO = 3       /* the density reduction                                             */
+  SGPU_KERNEL_PSI_RHO = 3,      /* the density reduction                                             */
+  SGPU_KERNEL_KB_FIELD = 4      /* the Kleinman-Bylander term at the sphere points from the projections */
 };
 
 /* Launches `kernel` reps times back to back on the handle's stream between two

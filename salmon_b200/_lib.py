@@ -41,9 +41,13 @@ ABI = {
     "sgpu_cg": (C.c_int, [_vp, _ip, _vp, _vp]),
     "sgpu_subspace_diag": (C.c_int, [_vp, _vp]),
     "sgpu_gs_to_rt": (C.c_int, [_vp]),
+    "sgpu_set_param": (C.c_int, [_vp, _ip, _ip]),
+    "sgpu_get_param": (C.c_int, [_vp, _ip, C.POINTER(C.c_int)]),
 }
 
-KERNELS = {"stencil_pass": 0, "taylor_last": 1, "uvpsi": 2, "psi_rho": 3}
+PARAMS = {"nslab": 0}
+
+KERNELS = {"stencil_pass": 0, "taylor_last": 1, "uvpsi": 2, "psi_rho": 3, "kb_field": 4}
 
 _LIB = None
 

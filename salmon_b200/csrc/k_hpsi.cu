@@ -1,5 +1,6 @@
-// Kleinman-Bylander projections and projector update for sm_100a, plus the
-// precision conversions.  The Hamiltonian pass itself is in k_pass.cu.
+// Kleinman-Bylander projections U, the KB field W at the sphere points and the
+// projector update for sm_100a, plus the precision conversions.  The
+// Hamiltonian pass itself is in k_pass.cu.
 #include <cuda_runtime.h>
 
 #include <type_traits>
@@ -48,6 +49,7 @@ __global__ void __launch_bounds__(32 * UV_WARPS) k_uvpsi(const C2<R>* __restrict
   for (int p = 0; p < 4; ++p)
 #pragma unroll
     for (int u = 0; u < UB; ++u) acc[p][u] = make_double2(0, 0);
+#pragma unroll 4
   for (int j = threadIdx.x; j < mps; j += 32 * UV_WARPS) {
     const int gi = __ldg(idx_proj + p0 + j);
     double2 v[UB];
@@ -123,6 +125,70 @@ cudaError_t launch_uvpsi_from_S(const System& s, const void* S, int o_beg, int n
     k_uvpsi<double><<<grid, 32 * UV_WARPS, 0, s.stream>>>((const double2*)S, nb, s.nsp, o_beg, nbk, s.zproj64, s.Nlma,
                                                           s.Nps, s.qmap, s.atom_off, s.items, s.lma_list, s.iuV_d,
                                                           s.Hxyz, scale_iuv ? 1 : 0, s.U);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------- KB field ---
+// W[b][q] = sum over the (ilma, j) entries of sphere point q of zproj(j,ilma,k) U[b][ilma]
+// (the dpseudo of pseudo_pt, common/hpsi.f90:194-200, already summed per grid
+// point), in entry order.  One thread per sphere point and KU orbitals; a
+// zproj value is loaded once for orbitals on the same k-point.
+constexpr int KU = 4;
+
+__device__ __forceinline__ int kb_entry(const int4& ra, const int4& rb, const int* cont, int e) {
+  if (e < 4) return e == 0 ? ra.z : (e == 1 ? ra.w : (e == 2 ? rb.x : rb.y));
+  return __ldg(cont + rb.z + (e - 4));
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_kbfield(const double2* __restrict__ U, int nb, int o_beg, int nbk,
+                                                 const C2<R>* __restrict__ zproj, int Nlma, int Nps,
+                                                 const int4* __restrict__ rec, const int* __restrict__ cont, int nsp,
+                                                 C2<R>* __restrict__ W) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  const int b0 = blockIdx.y * KU;
+  if (q >= nsp) return;
+  const int4 ra = __ldg(rec + 2 * (size_t)q), rb = __ldg(rec + 2 * (size_t)q + 1);
+  const int ne = ra.y + rb.w;
+  int kl[KU];
+  bool valid[KU];
+#pragma unroll
+  for (int u = 0; u < KU; ++u) {
+    valid[u] = b0 + u < nb;
+    kl[u] = valid[u] ? (o_beg + b0 + u) / nbk : 0;
+  }
+  bool samek = true;
+#pragma unroll
+  for (int u = 1; u < KU; ++u) samek = samek && (!valid[u] || kl[u] == kl[0]);
+  C2<R> acc[KU];
+#pragma unroll
+  for (int u = 0; u < KU; ++u) acc[u] = mk<R>(0, 0);
+  for (int e = 0; e < ne; ++e) {
+    const int en = kb_entry(ra, rb, cont, e);
+    const int ilma = en >> 16, zoff = ilma * Nps + (en & 0xffff);
+    C2<R> z0 = __ldg(zproj + (size_t)kl[0] * Nlma * Nps + zoff);
+#pragma unroll
+    for (int u = 0; u < KU; ++u) {
+      if (!valid[u]) continue;
+      const C2<R> z = samek ? z0 : __ldg(zproj + (size_t)kl[u] * Nlma * Nps + zoff);
+      const double2 uu = __ldg(U + (size_t)(b0 + u) * Nlma + ilma);
+      acc[u] = cfma(z, mk<R>((R)uu.x, (R)uu.y), acc[u]);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < KU; ++u)
+    if (valid[u]) W[(size_t)(b0 + u) * nsp + q] = acc[u];
+}
+
+cudaError_t launch_kbfield(const System& s, int o_beg, int nb, int nbk, void* W, int prec) {
+  if (s.nsp == 0 || nb == 0) return cudaSuccess;
+  dim3 grid((s.nsp + 255) / 256, (nb + KU - 1) / KU);
+  if ((prec < 0 ? s.prec : prec) == SGPU_PREC_C64)
+    k_kbfield<float><<<grid, 256, 0, s.stream>>>(s.U, nb, o_beg, nbk, s.zproj32, s.Nlma, s.Nps, s.rec, s.cont, s.nsp,
+                                                (float2*)W);
+  else
+    k_kbfield<double><<<grid, 256, 0, s.stream>>>(s.U, nb, o_beg, nbk, s.zproj64, s.Nlma, s.Nps, s.rec, s.cont, s.nsp,
+                                                 (double2*)W);
   return cudaGetLastError();
 }
 

@@ -76,6 +76,23 @@ int set_kac(System* s, const double* kAc) {
 
 int one_orbital_k(const System* s, int ik) { return (ik - s->NK_s) * s->NBocc; }
 
+// One H application of a batch: projections U (gathered from io.in, or from the
+// sphere values S exported by the previous pass), the KB field W at the sphere
+// points, then the stencil pass (which may export its output to S).
+cudaError_t apply_h(System* s, int mode, sgpu::PassIO io, int o_beg, int nb, int nbk, int prec, bool u_from_S) {
+  cudaError_t e;
+  if (u_from_S)
+    e = sgpu::launch_uvpsi_from_S(*s, s->Sbuf, o_beg, nb, nbk, true);
+  else
+    e = sgpu::launch_uvpsi(*s, io.in, o_beg, nb, nbk, true, prec);
+  if (e != cudaSuccess) return e;
+  if (s->nsp > 0) {
+    if ((e = sgpu::launch_kbfield(*s, o_beg, nb, nbk, s->Wbuf, prec)) != cudaSuccess) return e;
+    io.W = s->Wbuf;
+  }
+  return sgpu::launch_hpsi_pass(*s, mode, io, o_beg, nb, nbk, prec);
+}
+
 }  // namespace
 
 struct sgpu_system : public System {};
@@ -128,9 +145,6 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
     s->lap[0][n] = d->lapx[n]; s->lap[1][n] = d->lapy[n]; s->lap[2][n] = d->lapz[n];
     s->nab[0][n] = d->nabx[n]; s->nab[1][n] = d->naby[n]; s->nab[2][n] = d->nabz[n];
   }
-  s->cubic = true;
-  for (int n = 0; n < 5; ++n)
-    s->cubic = s->cubic && d->lapx[n] == d->lapy[n] && d->lapx[n] == d->lapz[n] && (n == 0 || (d->nabx[n] == d->naby[n] && d->nabx[n] == d->nabz[n]));
   s->NI = d->Nlma > 0 ? d->NI : 0;
   s->Nps = d->Nlma > 0 ? d->Nps : 0;
   s->Nlma = d->Nlma;
@@ -196,6 +210,7 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
   // packed projector points to sphere points
   std::vector<int> sp_off(s->NLx + 1, 0), q_of(s->NL, -1), qmap(std::max(1, s->NPI), 0);
   std::vector<int4> rec;
+  std::vector<int> cont;
   {
     if (s->Nps >= 65536 || s->Nlma >= 32768)
       return bail(fail(SGPU_ERR_UNSUPPORTED, "sgpu_create: Nps must be < 65536 and Nlma < 32768"));
@@ -206,23 +221,31 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
       for (int i = x * NYZ; i < (x + 1) * NYZ; ++i) {
         const int c = cnt[i + 1] - cnt[i];
         if (c == 0) continue;
-        if (c > 4)
-          return bail(fail(SGPU_ERR_UNSUPPORTED,
-                           "sgpu_create: a grid point lies in more than 4 projector spheres (entries per point > 4)"));
         int e[4] = {0, 0, 0, 0};
+        const int c0 = (int)cont.size();
         for (int k = 0; k < c; ++k) {
           const int2 en = ent[cnt[i] + k];  // {ilma*Nps + j, ilma}
-          e[k] = (en.y << 16) | (en.x - en.y * s->Nps);
+          const int ek = (en.y << 16) | (en.x - en.y * s->Nps);
+          if (k < 4) e[k] = ek;
+          else cont.push_back(ek);
         }
-        rec.push_back(make_int4(i - x * NYZ, c, e[0], e[1]));
-        rec.push_back(make_int4(e[2], e[3], 0, 0));
+        rec.push_back(make_int4(i - x * NYZ, std::min(c, 4), e[0], e[1]));
+        rec.push_back(make_int4(e[2], e[3], c0, std::max(c - 4, 0)));
         q_of[i] = nsp++;
       }
     }
     sp_off[s->NLx] = nsp;
     s->nsp = nsp;
+    for (int x = 0; x < s->NLx; ++x) s->maxpts = std::max(s->maxpts, sp_off[x + 1] - sp_off[x]);
     for (int p = 0; p < s->NPI; ++p) qmap[p] = q_of[idx_proj[p]];
+    if (s->maxpts > 32767) return bail(fail(SGPU_ERR_UNSUPPORTED, "sgpu_create: more than 32767 sphere points in one x-plane"));
   }
+  std::vector<short> lqi(s->NL, (short)-1);
+  for (int i = 0; i < s->NL; ++i)
+    if (q_of[i] >= 0) lqi[i] = (short)(q_of[i] - sp_off[i / (s->NLy * s->NLz)]);
+  for (int pr = 0; pr < 2; ++pr)
+    if (sgpu::pass_smem_bytes(pr, s->NLy, s->NLz, s->maxpts, true, s->NLx) > 227 * 1024)
+      return bail(fail(SGPU_ERR_UNSUPPORTED, "sgpu_create: an NLy x NLz plane ring does not fit in shared memory"));
   std::vector<double> uv((size_t)s->Nlma * s->Nps);
   if (s->Nlma) std::memcpy(uv.data(), d->uV, uv.size() * sizeof(double));
 
@@ -246,7 +269,9 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
   UP(s->uV_d, uv);
   UP(s->sp_off, sp_off);
   UP(s->rec, rec);
+  UP(s->cont, cont);
   UP(s->qmap, qmap);
+  UP(s->lqi, lqi);
   UP(s->occ_o, occo);
 #undef UP
   const size_t nz = (size_t)s->nkl * s->Nlma * s->Nps;
@@ -260,6 +285,9 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
   s->U_rows = (size_t)s->norb;
   if ((e = cudaMalloc(&s->Sbuf, (size_t)s->norb * std::max(1, s->nsp) * sizeof(double2))) != cudaSuccess)
     return bail(cuda_fail(e, "alloc S"));
+  if ((e = cudaMalloc(&s->Wbuf, (size_t)s->norb * std::max(1, s->nsp) * sizeof(double2))) != cudaSuccess)
+    return bail(cuda_fail(e, "alloc W"));
+  s->W_rows = (size_t)s->norb;
   if ((e = dalloc(&s->Uw, (size_t)s->norb * std::max(1, s->Nlma) * 4)) != cudaSuccess)
     return bail(cuda_fail(e, "alloc Uw"));
   if ((e = dalloc(&s->kAc_d, 3 * (size_t)s->nkl)) != cudaSuccess) return bail(cuda_fail(e, "alloc kAc"));
@@ -289,7 +317,7 @@ int sgpu_destroy(sgpu_handle h) {
   if (s->stream) cudaStreamSynchronize(s->stream);
   free_state_buffers(s);
   void* bufs[] = {s->vloc64, s->vloc32, s->occ_o, s->kAc_d, s->idx_proj, s->atom_off, s->rpos, s->items,
-                  s->lma_list, s->iuV_d, s->lma_atom, s->uV_d, s->zproj64, s->zproj32, s->sp_off, s->rec, s->qmap, s->Sbuf,
+                  s->lma_list, s->iuV_d, s->lma_atom, s->uV_d, s->zproj64, s->zproj32, s->sp_off, s->rec, s->cont, s->qmap, s->lqi, s->Sbuf, s->Wbuf,
                   s->U, s->Uw, s->red, s->stage};
   for (void* p : bufs) cudaFree(p);
   void* gbufs[] = {s->gs_zu, s->gs_aux, s->gs_W, s->gs_st, s->gs_part, s->gs_A, s->gs_V, s->gs_w, s->gs_sweeps,
@@ -416,21 +444,18 @@ int sgpu_hamiltonian(sgpu_handle h, double dt, int flag_current) {
   // projections read S instead of gathering from the full orbitals.
   const void* ins[4] = {s->zu, s->tw[0], s->tw[1], s->tw[2]};
   for (int n = 0; n < 4; ++n) {
-    if (n == 0 && !s->S_valid)
-      CK(sgpu::launch_uvpsi(*s, ins[0], 0, s->norb, s->NBocc, true));
-    else
-      CK(sgpu::launch_uvpsi_from_S(*s, s->Sbuf, 0, s->norb, s->NBocc, true));
     io.in = ins[n];
     io.S = s->nsp > 0 ? s->Sbuf : nullptr;
+    const bool from_S = s->nsp > 0 && (n > 0 || s->S_valid);
     if (n < 3) {
       io.out = s->tw[n];
-      CK(sgpu::launch_hpsi_pass(*s, 0, io, 0, s->norb, s->NBocc));
+      CK(apply_h(s, 0, io, 0, s->norb, s->NBocc, -1, from_S));
     } else {
       io.out = nullptr;
       io.t1 = s->tw[0];
       io.t2 = s->tw[1];
       io.zu = s->zu;
-      CK(sgpu::launch_hpsi_pass(*s, 2, io, 0, s->norb, s->NBocc));
+      CK(apply_h(s, 2, io, 0, s->norb, s->NBocc, -1, from_S));
     }
   }
   s->S_valid = s->nsp > 0;
@@ -456,14 +481,12 @@ int sgpu_hpsi(sgpu_handle h, int ik, const double* tpsi, double* htpsi, double* 
     float2* tt32 = (float2*)s->tw[2];
     CK(sgpu::launch_c128_to_c64(in128, in32, NL, s->stream));
     io.in = in32; io.out = out32; io.tt = tt32;
-    CK(sgpu::launch_uvpsi(*s, in32, ob, 1, s->NBocc, true));
-    CK(sgpu::launch_hpsi_pass(*s, ttpsi ? 1 : 0, io, ob, 1, s->NBocc));
+    CK(apply_h(s, ttpsi ? 1 : 0, io, ob, 1, s->NBocc, -1, false));
     CK(sgpu::launch_c64_to_c128(out32, out128, NL, s->stream));
     if (ttpsi) CK(sgpu::launch_c64_to_c128(tt32, tt128, NL, s->stream));
   } else {
     io.in = in128; io.out = out128; io.tt = tt128;
-    CK(sgpu::launch_uvpsi(*s, in128, ob, 1, s->NBocc, true));
-    CK(sgpu::launch_hpsi_pass(*s, ttpsi ? 1 : 0, io, ob, 1, s->NBocc));
+    CK(apply_h(s, ttpsi ? 1 : 0, io, ob, 1, s->NBocc, -1, false));
   }
   CK(cudaMemcpyAsync(htpsi, out128, NL * sizeof(double2), cudaMemcpyDeviceToHost, s->stream));
   if (ttpsi) CK(cudaMemcpyAsync(ttpsi, tt128, NL * sizeof(double2), cudaMemcpyDeviceToHost, s->stream));
@@ -482,8 +505,8 @@ int sgpu_hpsi_batch(sgpu_handle h, int ikb_s, int ikb_e, const void* tpsi, void*
   sgpu::PassIO io;
   io.in = tpsi;
   io.out = htpsi;
-  CK(sgpu::launch_uvpsi(*s, tpsi, ikb_s - 1, nb, s->NBocc, true));
-  CK(sgpu::launch_hpsi_pass(*s, 0, io, ikb_s - 1, nb, s->NBocc));
+  if ((size_t)nb > s->U_rows || (size_t)nb > s->W_rows) return fail(SGPU_ERR_ARG, "sgpu_hpsi_batch: batch too large");
+  CK(apply_h(s, 0, io, ikb_s - 1, nb, s->NBocc, -1, false));
   return 0;
 }
 
@@ -540,12 +563,15 @@ int sgpu_time_kernel(sgpu_handle h, int kernel, int reps, double* ms_per_launch)
   CK(cudaEventCreate(&e1));
   auto launch = [&]() -> cudaError_t {
     switch (kernel) {
-      case SGPU_KERNEL_STENCIL_PASS:  // as in the Taylor step: with the sphere-value export
-        io.in = s->zu; io.out = s->tw[0]; io.S = s->nsp > 0 ? s->Sbuf : nullptr;
+      case SGPU_KERNEL_STENCIL_PASS:  // as in the Taylor step: KB field added, sphere values exported
+        io.in = s->zu; io.out = s->tw[0]; io.S = s->nsp > 0 ? s->Sbuf : nullptr; io.W = s->nsp > 0 ? s->Wbuf : nullptr;
         return sgpu::launch_hpsi_pass(*s, 0, io, 0, s->norb, s->NBocc);
       case SGPU_KERNEL_TAYLOR_LAST:  // reads tw[2], tw[0], tw[1] and updates tw[2] in place (zu untouched)
-        io.in = s->tw[0]; io.t1 = s->tw[1]; io.t2 = s->tw[1]; io.zu = s->tw[2]; io.S = s->nsp > 0 ? s->Sbuf : nullptr;
+        io.in = s->tw[0]; io.t1 = s->tw[1]; io.t2 = s->tw[1]; io.zu = s->tw[2];
+        io.S = s->nsp > 0 ? s->Sbuf : nullptr; io.W = s->nsp > 0 ? s->Wbuf : nullptr;
         return sgpu::launch_hpsi_pass(*s, 2, io, 0, s->norb, s->NBocc);
+      case SGPU_KERNEL_KB_FIELD:
+        return sgpu::launch_kbfield(*s, 0, s->norb, s->NBocc, s->Wbuf);
       case SGPU_KERNEL_UVPSI:  // projections from the exported sphere values (passes 2-4 of a step)
         return sgpu::launch_uvpsi_from_S(*s, s->Sbuf, 0, s->norb, s->NBocc, true);
       case SGPU_KERNEL_PSI_RHO:
@@ -597,6 +623,13 @@ int gs_alloc(System* s) {
   CK(cudaMalloc(&s->occ_gs, occ.size() * sizeof(double)));
   CK(cudaMemcpyAsync(s->occ_gs, occ.data(), occ.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream));
   const size_t rows = std::max((size_t)s->norb, (size_t)s->nkl * s->NB);
+  if (rows > s->W_rows) {
+    CK(cudaStreamSynchronize(s->stream));
+    cudaFree(s->Wbuf);
+    s->Wbuf = nullptr;
+    CK(cudaMalloc(&s->Wbuf, rows * std::max(1, s->nsp) * sizeof(double2)));
+    s->W_rows = rows;
+  }
   if (rows > s->U_rows) {
     CK(cudaStreamSynchronize(s->stream));
     cudaFree(s->U);
@@ -614,8 +647,7 @@ int gs_hpsi(System* s, const double2* in, double2* out, double2* tt, int nb, int
   io.in = in;
   io.out = out;
   io.tt = tt;
-  CK(sgpu::launch_uvpsi(*s, in, 0, nb, nbk, true, SGPU_PREC_C128));
-  CK(sgpu::launch_hpsi_pass(*s, tt ? 1 : 0, io, 0, nb, nbk, SGPU_PREC_C128));
+  CK(apply_h(s, tt ? 1 : 0, io, 0, nb, nbk, SGPU_PREC_C128, false));
   return 0;
 }
 
@@ -737,3 +769,24 @@ int sgpu_gs_to_rt(sgpu_handle h) {
 }
 
 }  // extern "C"
+
+extern "C" int sgpu_set_param(sgpu_handle h, int param, int value) {
+  if (!valid(h)) return fail(SGPU_ERR_ARG, "null handle");
+  System* s = h;
+  switch (param) {
+    case SGPU_PARAM_NSLAB:
+      if (value < 1 || value > s->NLx) return fail(SGPU_ERR_ARG, "sgpu_set_param: nslab must be in 1..NLx");
+      s->nslab = value;
+      return 0;
+    default:
+      return fail(SGPU_ERR_ARG, "sgpu_set_param: unknown parameter");
+  }
+}
+
+extern "C" int sgpu_get_param(sgpu_handle h, int param, int* value) {
+  if (!valid(h) || !value) return fail(SGPU_ERR_ARG, "sgpu_get_param: null argument");
+  switch (param) {
+    case SGPU_PARAM_NSLAB: *value = h->nslab; return 0;
+    default: return fail(SGPU_ERR_ARG, "sgpu_get_param: unknown parameter");
+  }
+}

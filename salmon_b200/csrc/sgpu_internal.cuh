@@ -100,17 +100,22 @@ struct System {
   double2* zproj64 = nullptr;      // [nkl][Nlma][Nps]
   float2* zproj32 = nullptr;       // [nkl][Nlma][Nps]   (C64 mode)
   // Kleinman-Bylander sphere points sorted by grid index: plane x holds points
-  // sp_off[x] .. sp_off[x+1]-1; point q has the record rec[2q..2q+1] =
-  // {in-plane position, entry count (<= 4), e0, e1}, {e2, e3, 0, 0} with
-  // e = ilma<<16 | j (zproj(j,ilma)).  qmap[p] is the sphere-point index of
-  // packed projector point p (the gather index into a sphere-value array S).
+  // sp_off[x] .. sp_off[x+1]-1 (at most maxpts); point q has the record
+  // rec[2q..2q+1] = {in-plane position, count of the first <= 4 entries, e0, e1},
+  // {e2, e3, first continuation, continuation count} with e = ilma<<16 | j
+  // (zproj(j,ilma)).  lqi[i] is grid point i's index among its plane's sphere
+  // points (-1 if none).  qmap[p] is the sphere-point index of packed projector
+  // point p (the gather index into a sphere-value array S).
   int* sp_off = nullptr;           // [NLx+1]
   int4* rec = nullptr;             // [2*nsp]
+  int* cont = nullptr;             // entries beyond the 4th of points in several spheres
   int* qmap = nullptr;             // [NPI]
-  int nsp = 0;
+  short* lqi = nullptr;            // [NL]
+  int nsp = 0, maxpts = 0;
+  void* Wbuf = nullptr;            // [W_rows][nsp] KB field (element: complex(8) capacity)
+  size_t W_rows = 0;
   void* Sbuf = nullptr;            // [norb][nsp] orbital values at the sphere points
   bool S_valid = false;            // Sbuf holds the sphere values of the resident zu
-  bool cubic = false;               // lapx==lapy==lapz and nabx==naby==nabz (packed FP32 pass)
   double2* U = nullptr;            // [norb][Nlma] projections <uV e^{ikr}|psi> (scaled)
   double2* Uw = nullptr;           // [norb][Nlma][4] weighted projections for the current
 
@@ -155,6 +160,10 @@ struct System {
 cudaError_t launch_uvpsi(const System& s, const void* in, int o_beg, int nb, int nbk, bool scale_iuv, int prec = -1);
 // the same projections from sphere values S[b][nsp] exported by a pass
 cudaError_t launch_uvpsi_from_S(const System& s, const void* S, int o_beg, int nb, int nbk, bool scale_iuv);
+// W[b][q] = sum_entries zproj U[b] at every sphere point (needs U of the batch)
+cudaError_t launch_kbfield(const System& s, int o_beg, int nb, int nbk, void* W, int prec = -1);
+// dynamic shared memory of the pass kernel
+size_t pass_smem_bytes(int prec, int NLy, int NLz, int maxpts, bool with_w, int NLx);
 
 // One H application: out = H in  (mode 0), with ttpsi (mode 1), or the last
 // Taylor pass (mode 2): zu = zu + z1 t1 + z2 t2 + z3 in + z4 H in.  U must hold
@@ -166,6 +175,7 @@ struct PassIO {
   const void* t1 = nullptr;
   const void* t2 = nullptr;
   void* zu = nullptr;
+  const void* W = nullptr;         // KB term at the sphere points ([nb][nsp]) or null (no projectors)
   void* S = nullptr;               // export of the output at the sphere points ([nb][nsp]) or null
   double zfac[4][2] = {};
 };

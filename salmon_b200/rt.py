@@ -122,6 +122,14 @@ class GpuSystem:
     def hpsi_batch(self, ikb_s: int, ikb_e: int, tpsi_dev: int, htpsi_dev: int):
         call("sgpu_hpsi_batch", self._h, ikb_s, ikb_e, C.c_void_p(tpsi_dev), C.c_void_p(htpsi_dev))
 
+    def set_param(self, name: str, value: int):
+        call("sgpu_set_param", self._h, _lib.PARAMS[name], int(value))
+
+    def get_param(self, name: str) -> int:
+        v = C.c_int()
+        call("sgpu_get_param", self._h, _lib.PARAMS[name], C.byref(v))
+        return v.value
+
     def time_kernel(self, kernel: str, reps: int = 10) -> float:
         """Mean device milliseconds per launch of one library kernel (CUDA events on the library stream)."""
         ms = C.c_double()
