@@ -170,6 +170,29 @@ int sgpu_hpsi_batch(sgpu_handle h, int ikb_s, int ikb_e, const void* tpsi, void*
  * (common/psi_rho.f90:47-90, sym1 :181-206). */
 int sgpu_psi_rho(sgpu_handle h, double* rho_l);
 
+/* Capacity of the fixed scratch of sgpu_psi_rho_static, in doubles (16 MiB):
+ * ceil(nb*nk/64) * NL must not exceed it (e.g. NL = 32^3 with up to 4096
+ * orbitals, or NL = 48^3 with up to 1152). */
+#define SGPU_PSI_RHO_STATIC_SCRATCH_DOUBLES 2097152
+
+/* rho(NL) = sum_{ik<nk, ib<nb} occ[ib + ld_occ*ik] |zu(:,ib,ik)|^2 (FP64) over
+ * orbitals the CALLER keeps on the device: zu(NL,nb,nk) complex(8)
+ * (precision SGPU_PREC_C128) or complex(4) (SGPU_PREC_C64), occ and rho
+ * device arrays; enqueued on `stream` (a cudaStream_t, NULL = the legacy
+ * default stream) and not waited for.  Needs no handle and allocates no
+ * device memory: its scratch is a static device array of
+ * SGPU_PSI_RHO_STATIC_SCRATCH_DOUBLES doubles, and larger problems are
+ * rejected with SGPU_ERR_ARG.  It is meant for hosts that own the orbitals
+ * through their own device runtime and cannot allocate at that point.
+ * The first call on each device looks up the scratch address
+ * (cudaGetSymbolAddress), so make it before capturing any stream.  All calls
+ * on one device share the scratch: calls whose executions overlap race, so
+ * order them (one stream, or events).
+ * No counterpart in the reference; the computation is psi_rho_impl with
+ * Sym=1 (common/psi_rho.f90:47-90, sym1 :181-206), like sgpu_psi_rho. */
+int sgpu_psi_rho_static(int precision, int NL, int nb, int nk, const void* zu, const double* occ, int ld_occ,
+                        double* rho, void* stream);
+
 /* Macroscopic current of the resident orbitals at k+A = kAc (HOST (NK,3));
  * jav(3) HOST, before the allreduce.  Rebuilds the projectors for kAc, as
  * current() does.  Replaces current('RT',...) impl

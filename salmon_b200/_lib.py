@@ -32,6 +32,7 @@ ABI = {
     "sgpu_hpsi": (C.c_int, [_vp, _ip, _vp, _vp, _vp]),
     "sgpu_hpsi_batch": (C.c_int, [_vp, _ip, _ip, _vp, _vp]),
     "sgpu_psi_rho": (C.c_int, [_vp, _vp]),
+    "sgpu_psi_rho_static": (C.c_int, [_ip, _ip, _ip, _ip, _vp, _vp, _ip, _vp, _vp]),
     "sgpu_current": (C.c_int, [_vp, _vp, _vp]),
     "sgpu_energy_terms": (C.c_int, [_vp, _vp, _dp, _dp]),
     "sgpu_time_kernel": (C.c_int, [_vp, _ip, _ip, _dp]),

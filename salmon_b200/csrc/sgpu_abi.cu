@@ -97,6 +97,9 @@ cudaError_t apply_h(System* s, int mode, sgpu::PassIO io, int o_beg, int nb, int
 
 struct sgpu_system : public System {};
 
+// Entry points defined in other files report through the same message slot.
+void sgpu::set_last_error(const std::string& msg) { g_err = msg; }
+
 extern "C" {
 
 const char* sgpu_last_error(void) { return g_err.c_str(); }

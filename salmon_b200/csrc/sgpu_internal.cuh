@@ -214,4 +214,7 @@ cudaError_t launch_subspace_h(const System& s, const double2* U, const double2* 
 cudaError_t launch_jacobi(const System& s, double2* A, double2* V, int max_sweeps, double* w, int* sweeps);
 cudaError_t launch_rotate(const System& s, const double2* in, const double2* Z, double2* out);
 
+// Sets the message that sgpu_last_error returns (defined with the C ABI).
+void set_last_error(const std::string& msg);
+
 }  // namespace sgpu
