@@ -190,7 +190,8 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
 
   // plane jn (relative to x_beg) into ring slot jn % NR, with its W chunk
   auto refill = [&](int jn) {
-    const int p = wrapi(x_beg + jn, a.NLx);
+    int p = x_beg + jn;
+    while (p >= a.NLx) p -= a.NLx;
     if (act && jn < nplanes) cp_run<R, RZ>(ring + (size_t)(jn % NR) * NYZ + own, inb + (size_t)p * NYZ + own);
     if (with_w && jn < nown) {
       const int q0 = spo[p], q1 = spo[p + 1];
@@ -213,7 +214,9 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
 #pragma unroll
   for (int m = 0; m < NZZ / RZ; ++m) zoff[m] = y * NLz + wrapi(z0 + m * RZ - 4, NLz);
 
-  // register queue: q[m] = this thread's points of plane x-4+m
+  // register queue: in the march step of phase P (plane x = x_beg + 9i + P),
+  // plane x-4+m sits in q[(P+m) % 9]; the march is unrolled nine times so the
+  // queue rotates by renaming, without register moves.
   T q[9][RZ];
   if (act) {
 #pragma unroll
@@ -229,7 +232,9 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
     if (with_w || do_export) ld_lq<RZ>(lq, a.lqi + (size_t)x_beg * NYZ + own);
   }
 
-  for (int x = x_beg; x < x_end; ++x) {
+  int x = x_beg;
+  auto step = [&](auto phase) -> bool {
+    constexpr int P = decltype(phase)::value;
     const int j = x - x_beg;
     cp_async_wait<NR - 6>();  // this thread's copies of planes <= x+4 have landed
     __syncthreads();          // ... and everyone's; the slot of plane x-1 is free
@@ -237,11 +242,13 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
     const T* pl = ring + (size_t)(j % NR) * NYZ;
     const bool more = x + 1 < x_end;
     if (act) {
-      if (j == 0) {
+      if constexpr (P == 0) {
+        if (j == 0) {
 #pragma unroll
-        for (int n = 4; n < 8; ++n) lds_run<R, RZ>(q[n], ring + (size_t)(n - 4) * NYZ + own);
+          for (int n = 4; n < 8; ++n) lds_run<R, RZ>(q[n], ring + (size_t)(n - 4) * NYZ + own);
+        }
       }
-      lds_run<R, RZ>(q[8], ring + (size_t)((j + 4) % NR) * NYZ + own);
+      lds_run<R, RZ>(q[(P + 8) % 9], ring + (size_t)((j + 4) % NR) * NYZ + own);
       const size_t pbase = (size_t)x * NYZ + own;
       R vln[RZ];
       int lqn[RZ];
@@ -260,7 +267,7 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
         T run[RZ];
         if (m * RZ == 4) {
 #pragma unroll
-          for (int s2 = 0; s2 < RZ; ++s2) run[s2] = q[4][s2];
+          for (int s2 = 0; s2 < RZ; ++s2) run[s2] = q[(P + 4) % 9][s2];
         } else {
           lds_run<R, RZ>(run, pl + zoff[m]);
         }
@@ -305,11 +312,11 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
       for (int n = 1; n <= 4; ++n)  // x: the register queue
 #pragma unroll
         for (int r = 0; r < RZ; ++r) {
-          const T p = q[4 + n][r], mm = q[4 - n][r];
-          v[r].x = fma(a.lapt[n - 1], p.x + mm.x, v[r].x);
-          v[r].y = fma(a.lapt[n - 1], p.y + mm.y, v[r].y);
-          wa[r].x = fma(a.nabc[n - 1], p.x - mm.x, wa[r].x);
-          wa[r].y = fma(a.nabc[n - 1], p.y - mm.y, wa[r].y);
+          const T pp = q[(P + 4 + n) % 9][r], mm = q[(P + 4 - n) % 9][r];
+          v[r].x = fma(a.lapt[n - 1], pp.x + mm.x, v[r].x);
+          v[r].y = fma(a.lapt[n - 1], pp.y + mm.y, v[r].y);
+          wa[r].x = fma(a.nabc[n - 1], pp.x - mm.x, wa[r].x);
+          wa[r].y = fma(a.nabc[n - 1], pp.y - mm.y, wa[r].y);
         }
 #pragma unroll
       for (int r = 0; r < RZ; ++r) {
@@ -321,7 +328,7 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
       T res[RZ];
 #pragma unroll
       for (int r = 0; r < RZ; ++r) {
-        const T c = q[4][r];
+        const T c = q[(P + 4) % 9][r];
         // F = B E + A E - 0.5 v - zI w   (stencil/F90/hpsi.f90:190)
         T f;
         f.x = fma(vl[r] + A, c.x, fma((R)-0.5, v[r].x, w[r].y));
@@ -342,7 +349,7 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
           T u = ps[r];
           u = cfma(a.zf[0], p1[r], u);
           u = cfma(a.zf[1], p2[r], u);
-          u = cfma(a.zf[2], q[4][r], u);
+          u = cfma(a.zf[2], q[(P + 4) % 9][r], u);
           u = cfma(a.zf[3], res[r], u);
           res[r] = u;
         }
@@ -358,11 +365,20 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
       }
 #pragma unroll
       for (int r = 0; r < RZ; ++r) { vl[r] = vln[r]; lq[r] = lqn[r]; }
-#pragma unroll
-      for (int n = 0; n < 8; ++n)
-#pragma unroll
-        for (int r = 0; r < RZ; ++r) q[n][r] = q[n + 1][r];
     }
+    ++x;
+    return x < x_end;
+  };
+  for (;;) {
+    if (!step(std::integral_constant<int, 0>{})) break;
+    if (!step(std::integral_constant<int, 1>{})) break;
+    if (!step(std::integral_constant<int, 2>{})) break;
+    if (!step(std::integral_constant<int, 3>{})) break;
+    if (!step(std::integral_constant<int, 4>{})) break;
+    if (!step(std::integral_constant<int, 5>{})) break;
+    if (!step(std::integral_constant<int, 6>{})) break;
+    if (!step(std::integral_constant<int, 7>{})) break;
+    if (!step(std::integral_constant<int, 8>{})) break;
   }
   cp_async_wait<0>();
 }
