@@ -35,9 +35,10 @@ sys.path.insert(0, ROOT)
 
 METRIC = "RT orbital-updates/s: FP32+FP64-reduce vs FP64 GPU at ΔJ<1e-5; hpsi %HBM peak"
 DT = 0.08
-# ncu dram__bytes_{read,write}.sum of the stencil pass, per launch, from the
-# capture summarised in profiles/ (None until a capture exists for the config).
-NCU_TRAFFIC_BYTES = {}
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of one stencil-pass launch, per
+# orbital, from the capture in profiles/k_hpsi_pass_uvpsi_kbfield_c64_32cubed_864orb.md
+# (864 orbitals; traffic grows with the orbital count).
+NCU_TRAFFIC_BYTES_PER_ORBITAL = {("stencil_pass", "c64", 32): 536.171264e6 / 864}
 
 
 def parse():
@@ -53,6 +54,7 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--only", choices=["c128", "c64"], help="run one precision (profiling)")
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling)")
+    p.add_argument("--no-precision", action="store_true", help="skip the FP32-vs-FP64 J(t) run")
     return p.parse_args()
 
 
@@ -156,6 +158,40 @@ def cpu_baseline(sysm, kAc, vloc, zu, seconds):
                       f"OpenMP over orbitals, complex(8)"}
 
 
+def precision_check(nsteps=500):
+    """J(t) of the complex(4) path against the complex(8) path: 16^3 grid, 4x4x4 k,
+    16 bands (the Si8 RT shape), ground state from GPU CG at fixed V_loc, impulsive
+    kick A_x = 1e-3, dt = 0.08, `nsteps` middle-point Taylor steps, J after each."""
+    from salmon_b200 import drive, system as S
+    from salmon_b200.rt import GpuSystem
+    sysm, _, vloc, zu = S.microbench_system(16, nkgrid=(4, 4, 4), Nb=16)
+    kAc0 = np.ascontiguousarray(sysm.kAc0)
+    with GpuSystem(sysm) as g:
+        g.set_vloc(vloc)
+        g.update_projector(kAc0)
+        g.gs_set_state(zu)
+        _, esp_var, hist = drive.ground_state(g, n_iter=40, ncg=4)
+        zgs = g.gs_get_state()
+    Ac = drive.init_Ac(nsteps, DT, "impulse", epdir=(1.0, 0.0, 0.0), e_impulse=1e-3)
+    out = {}
+    for prec in ("c128", "c64"):
+        with GpuSystem(sysm, "c128") as g:
+            g.set_vloc(vloc)
+            g.update_projector(kAc0)
+            g.gs_set_state(zgs)
+            g.gs_to_rt()
+            if prec == "c64":
+                g.set_precision("c64")
+            out[prec] = drive.rt_propagate(g, sysm, kAc0, vloc, Ac, DT, nsteps, energy_every=50)
+    (j64, e64), (j32, e32) = out["c128"], out["c64"]
+    de = max(abs((e32[t] - e32[0]) - (e64[t] - e64[0])) for t in e64)
+    return {"j_rel_err": drive.j_error(j64, j32), "j_dyn_rel_err": drive.j_error_dynamic(j64, j32),
+            "max_abs_j_fp64": float(np.abs(j64).max()), "band_energy_change_abs_diff_ha": de,
+            "gs_max_residual": float(esp_var.max()),
+            "workload": f"16^3, 64 k x 16 bands, impulse A_x=1e-3, dt={DT}, {nsteps} steps, fixed V_loc, "
+                        "J every step (FP64 reductions)", "target": 1e-5}
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -236,10 +272,12 @@ def main():
         ctx = Clocks(local) if prec == "c64" else None
         if ctx:
             ctx.__enter__()
+        g.set_param("launches", 0)
         e0.record(stream)
         for _ in range(args.steps):
             g.hamiltonian(DT)
         e1.record(stream)
+        launches = g.get_param("launches")
         e1.synchronize()
         if ctx:
             ctx.__exit__(None, None, None)
@@ -247,7 +285,7 @@ def main():
         barrier()
         torch.cuda.synchronize()
         ms = max_over_ranks(e0.elapsed_time(e1))
-        r = {"ms_per_step": ms / args.steps, "value": norb * world * args.steps / (ms / 1000.0)}
+        r = {"ms_per_step": ms / args.steps, "value": norb * world * args.steps / (ms / 1000.0), "launches": launches}
         # dominant kernel: one H application of all orbitals (stencil + KB scatter), events on its stream
         t_pass = g.time_kernel("stencil_pass", reps=10)
         t_last = g.time_kernel("taylor_last", reps=5)
@@ -284,6 +322,9 @@ def main():
         g.close()
         del stream
 
+    prec_check = None
+    if rank == 0 and not (args.only or args.no_e2e or args.no_precision):
+        prec_check = precision_check()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -294,7 +335,8 @@ def main():
         print(json.dumps({p: {k: v for k, v in r.items() if k != "e2e"} for p, r in res.items()}))
     elif rank == 0:
         h = res["c64"]
-        traffic = NCU_TRAFFIC_BYTES.get(("stencil_pass", "c64", args.grid))
+        tpo = NCU_TRAFFIC_BYTES_PER_ORBITAL.get(("stencil_pass", "c64", args.grid))
+        traffic = tpo * norb if tpo else None
         out = {
             "metric": METRIC, "value": h["value"], "unit": "orbital-updates/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": h["ms_per_step"], "higher_is_better": True, "scaling": "weak",
@@ -315,7 +357,8 @@ def main():
                          "peak_kind": peak_kind},
             "cpu_baseline": cpu,
             "e2e": h["e2e"],
-            "gpu_launches": args.steps * 8 * 1,
+            "gpu_launches": h["launches"],
+            "precision": prec_check,
             "clocks": clocks,
         }
         print(json.dumps(out))

@@ -239,7 +239,8 @@ int sgpu_gs_to_rt(sgpu_handle h);
 
 /* ---- tuning --------------------------------------------------------------- */
 enum {
-  SGPU_PARAM_NSLAB = 0   /* CTAs per orbital along x in the stencil pass (1..NLx) */
+  SGPU_PARAM_NSLAB = 0,   /* CTAs per orbital along x in the stencil pass (1..NLx) */
+  SGPU_PARAM_LAUNCHES = 1 /* kernels the handle has launched, modulo 2^31 (read; set to 0 to reset) */
 };
 
 /* Sets / reads a launch parameter of the handle (the autotuner's knobs).  No

@@ -46,7 +46,7 @@ ABI = {
     "sgpu_get_param": (C.c_int, [_vp, _ip, C.POINTER(C.c_int)]),
 }
 
-PARAMS = {"nslab": 0}
+PARAMS = {"nslab": 0, "launches": 1}
 
 KERNELS = {"stencil_pass": 0, "taylor_last": 1, "uvpsi": 2, "psi_rho": 3, "kb_field": 4}
 

@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(GS_THREADS) k_gram_schmidt(double2* __restrict
 }
 
 cudaError_t launch_gram_schmidt(const System& s, double2* zu) {
-  k_gram_schmidt<<<s.nkl, GS_THREADS, 0, s.stream>>>(zu, s.NB, s.NL, s.Hxyz);
+  k_gram_schmidt<<<s.nkl, GS_THREADS, 0, s.launch_stream()>>>(zu, s.NB, s.NL, s.Hxyz);
   return cudaGetLastError();
 }
 
@@ -207,27 +207,27 @@ __global__ void __launch_bounds__(GS_THREADS) k_cg_resid(double2* __restrict__ W
 }
 
 cudaError_t launch_cg_begin(const System& s, double2* zu, double2* W, void* st, int ib) {
-  k_cg_begin<<<s.nkl, GS_THREADS, 0, s.stream>>>(zu, W, (CGState*)st, ib, s.NB, s.NL, s.Hxyz);
+  k_cg_begin<<<s.nkl, GS_THREADS, 0, s.launch_stream()>>>(zu, W, (CGState*)st, ib, s.NB, s.NL, s.Hxyz);
   return cudaGetLastError();
 }
 cudaError_t launch_cg_dot0(const System& s, double2* W, void* st) {
-  k_cg_dot0<<<s.nkl, GS_THREADS, 0, s.stream>>>(W, (CGState*)st, s.NL, s.Hxyz);
+  k_cg_dot0<<<s.nkl, GS_THREADS, 0, s.launch_stream()>>>(W, (CGState*)st, s.NL, s.Hxyz);
   return cudaGetLastError();
 }
 cudaError_t launch_cg_pre(const System& s, const double2* zu, double2* W, void* st, int ib, int iter) {
-  k_cg_pre<<<s.nkl, GS_THREADS, 0, s.stream>>>(zu, W, (CGState*)st, ib, iter, s.NB, s.NL, s.Hxyz);
+  k_cg_pre<<<s.nkl, GS_THREADS, 0, s.launch_stream()>>>(zu, W, (CGState*)st, ib, iter, s.NB, s.NL, s.Hxyz);
   return cudaGetLastError();
 }
 cudaError_t launch_cg_post(const System& s, double2* W, void* st, int iter) {
-  k_cg_post<<<s.nkl, GS_THREADS, 0, s.stream>>>(W, (CGState*)st, iter, s.NL, s.Hxyz);
+  k_cg_post<<<s.nkl, GS_THREADS, 0, s.launch_stream()>>>(W, (CGState*)st, iter, s.NL, s.Hxyz);
   return cudaGetLastError();
 }
 cudaError_t launch_cg_end(const System& s, double2* zu, double2* W, int ib) {
-  k_cg_end<<<s.nkl, GS_THREADS, 0, s.stream>>>(zu, W, ib, s.NB, s.NL, s.Hxyz);
+  k_cg_end<<<s.nkl, GS_THREADS, 0, s.launch_stream()>>>(zu, W, ib, s.NB, s.NL, s.Hxyz);
   return cudaGetLastError();
 }
 cudaError_t launch_cg_resid(const System& s, double2* W, const double* occ_gs, double* esp_var, int ib) {
-  k_cg_resid<<<s.nkl, GS_THREADS, 0, s.stream>>>(W, occ_gs, esp_var, ib, s.NB, s.NL, s.Hxyz);
+  k_cg_resid<<<s.nkl, GS_THREADS, 0, s.launch_stream()>>>(W, occ_gs, esp_var, ib, s.NB, s.NL, s.Hxyz);
   return cudaGetLastError();
 }
 size_t cg_state_bytes() { return sizeof(CGState); }
@@ -295,11 +295,11 @@ cudaError_t launch_subspace_h(const System& s, const double2* U, const double2* 
   const int nt = (s.NB + GT - 1) / GT;
   const int kchunk = ((s.NL + nsplit - 1) / nsplit + GK - 1) / GK * GK;
   dim3 grid(s.nkl * nt, nt, nsplit);
-  k_zgemm_hn<<<grid, GT * GT, 0, s.stream>>>(U, HU, s.NB, s.NL, kchunk, part);
+  k_zgemm_hn<<<grid, GT * GT, 0, s.launch_stream()>>>(U, HU, s.NB, s.NL, kchunk, part);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const size_t tot = (size_t)s.nkl * s.NB * s.NB;
-  k_zgemm_reduce_herm<<<(int)std::min<size_t>((tot + 255) / 256, 4096), 256, 0, s.stream>>>(part, nsplit, s.nkl, s.NB,
+  k_zgemm_reduce_herm<<<(int)std::min<size_t>((tot + 255) / 256, 4096), 256, 0, s.launch_stream()>>>(part, nsplit, s.nkl, s.NB,
                                                                                              s.Hxyz, za);
   return cudaGetLastError();
 }
@@ -431,7 +431,7 @@ __global__ void __launch_bounds__(1024) k_jacobi_herm(double2* __restrict__ Aall
 
 cudaError_t launch_jacobi(const System& s, double2* A, double2* V, int max_sweeps, double* w, int* sweeps) {
   const size_t smem = (size_t)s.NB * (4 * sizeof(double) + sizeof(int));
-  k_jacobi_herm<<<s.nkl, 1024, smem, s.stream>>>(A, V, s.NB, max_sweeps, w, sweeps);
+  k_jacobi_herm<<<s.nkl, 1024, smem, s.launch_stream()>>>(A, V, s.NB, max_sweeps, w, sweeps);
   return cudaGetLastError();
 }
 
@@ -464,7 +464,7 @@ __global__ void __launch_bounds__(256) k_rotate(const double2* __restrict__ in, 
 
 cudaError_t launch_rotate(const System& s, const double2* in, const double2* Z, double2* out) {
   dim3 grid((s.NL + 255) / 256, s.nkl);
-  k_rotate<<<grid, 256, 0, s.stream>>>(in, Z, s.NB, s.NL, out);
+  k_rotate<<<grid, 256, 0, s.launch_stream()>>>(in, Z, s.NB, s.NL, out);
   return cudaGetLastError();
 }
 

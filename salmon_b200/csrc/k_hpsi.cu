@@ -104,11 +104,11 @@ cudaError_t launch_uvpsi(const System& s, const void* in, int o_beg, int nb, int
   if (s.Nlma == 0 || nb == 0) return cudaSuccess;
   dim3 grid((nb + UB - 1) / UB, s.nitems);
   if ((prec < 0 ? s.prec : prec) == SGPU_PREC_C64)
-    k_uvpsi<float><<<grid, 32 * UV_WARPS, 0, s.stream>>>((const float2*)in, nb, s.NL, o_beg, nbk, s.zproj64, s.Nlma,
+    k_uvpsi<float><<<grid, 32 * UV_WARPS, 0, s.launch_stream()>>>((const float2*)in, nb, s.NL, o_beg, nbk, s.zproj64, s.Nlma,
                                                          s.Nps, s.idx_proj, s.atom_off, s.items, s.lma_list, s.iuV_d,
                                                          s.Hxyz, scale_iuv ? 1 : 0, s.U);
   else
-    k_uvpsi<double><<<grid, 32 * UV_WARPS, 0, s.stream>>>((const double2*)in, nb, s.NL, o_beg, nbk, s.zproj64, s.Nlma,
+    k_uvpsi<double><<<grid, 32 * UV_WARPS, 0, s.launch_stream()>>>((const double2*)in, nb, s.NL, o_beg, nbk, s.zproj64, s.Nlma,
                                                           s.Nps, s.idx_proj, s.atom_off, s.items, s.lma_list, s.iuV_d,
                                                           s.Hxyz, scale_iuv ? 1 : 0, s.U);
   return cudaGetLastError();
@@ -118,11 +118,11 @@ cudaError_t launch_uvpsi_from_S(const System& s, const void* S, int o_beg, int n
   if (s.Nlma == 0 || nb == 0) return cudaSuccess;
   dim3 grid((nb + UB - 1) / UB, s.nitems);
   if (s.prec == SGPU_PREC_C64)
-    k_uvpsi<float><<<grid, 32 * UV_WARPS, 0, s.stream>>>((const float2*)S, nb, s.nsp, o_beg, nbk, s.zproj64, s.Nlma,
+    k_uvpsi<float><<<grid, 32 * UV_WARPS, 0, s.launch_stream()>>>((const float2*)S, nb, s.nsp, o_beg, nbk, s.zproj64, s.Nlma,
                                                          s.Nps, s.qmap, s.atom_off, s.items, s.lma_list, s.iuV_d,
                                                          s.Hxyz, scale_iuv ? 1 : 0, s.U);
   else
-    k_uvpsi<double><<<grid, 32 * UV_WARPS, 0, s.stream>>>((const double2*)S, nb, s.nsp, o_beg, nbk, s.zproj64, s.Nlma,
+    k_uvpsi<double><<<grid, 32 * UV_WARPS, 0, s.launch_stream()>>>((const double2*)S, nb, s.nsp, o_beg, nbk, s.zproj64, s.Nlma,
                                                           s.Nps, s.qmap, s.atom_off, s.items, s.lma_list, s.iuV_d,
                                                           s.Hxyz, scale_iuv ? 1 : 0, s.U);
   return cudaGetLastError();
@@ -184,10 +184,10 @@ cudaError_t launch_kbfield(const System& s, int o_beg, int nb, int nbk, void* W,
   if (s.nsp == 0 || nb == 0) return cudaSuccess;
   dim3 grid((s.nsp + 255) / 256, (nb + KU - 1) / KU);
   if ((prec < 0 ? s.prec : prec) == SGPU_PREC_C64)
-    k_kbfield<float><<<grid, 256, 0, s.stream>>>(s.U, nb, o_beg, nbk, s.zproj32, s.Nlma, s.Nps, s.rec, s.cont, s.nsp,
+    k_kbfield<float><<<grid, 256, 0, s.launch_stream()>>>(s.U, nb, o_beg, nbk, s.zproj32, s.Nlma, s.Nps, s.rec, s.cont, s.nsp,
                                                 (float2*)W);
   else
-    k_kbfield<double><<<grid, 256, 0, s.stream>>>(s.U, nb, o_beg, nbk, s.zproj64, s.Nlma, s.Nps, s.rec, s.cont, s.nsp,
+    k_kbfield<double><<<grid, 256, 0, s.launch_stream()>>>(s.U, nb, o_beg, nbk, s.zproj64, s.Nlma, s.Nps, s.rec, s.cont, s.nsp,
                                                  (double2*)W);
   return cudaGetLastError();
 }
@@ -221,7 +221,7 @@ __global__ void k_update_projector(const double* __restrict__ kAc, const double*
 cudaError_t launch_update_projector(const System& s) {
   if (s.Nlma == 0) return cudaSuccess;
   dim3 grid(s.Nlma, s.nkl);
-  k_update_projector<<<grid, 128, 0, s.stream>>>(s.kAc_d, s.rpos, s.atom_off, s.lma_atom, s.uV_d, s.Nlma, s.Nps,
+  k_update_projector<<<grid, 128, 0, s.launch_stream()>>>(s.kAc_d, s.rpos, s.atom_off, s.lma_atom, s.uV_d, s.Nlma, s.Nps,
                                                  s.zproj64, s.prec == SGPU_PREC_C64 ? s.zproj32 : nullptr);
   return cudaGetLastError();
 }

@@ -423,7 +423,7 @@ static cudaError_t launch_pass_t(const System& s, const PassIO& io, int o_beg, i
     if (e != cudaSuccess) return e;
   }
   dim3 grid(nb, (s.NLx + a.SX - 1) / a.SX);
-  kern<<<grid, block, smem, s.stream>>>(a);
+  kern<<<grid, block, smem, s.launch_stream()>>>(a);
   return cudaGetLastError();
 }
 

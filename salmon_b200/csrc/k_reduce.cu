@@ -49,10 +49,10 @@ cudaError_t launch_psi_rho(System& s, double* rho_dev) {
   if ((size_t)nchunk * s.NL > s.red_elems) return cudaErrorInvalidValue;
   dim3 grid((s.NL + 255) / 256, nchunk);
   if (s.prec == SGPU_PREC_C64)
-    k_rho_partial<float><<<grid, 256, 0, s.stream>>>((const float2*)s.zu, s.occ_o, s.norb, s.NL, s.red);
+    k_rho_partial<float><<<grid, 256, 0, s.launch_stream()>>>((const float2*)s.zu, s.occ_o, s.norb, s.NL, s.red);
   else
-    k_rho_partial<double><<<grid, 256, 0, s.stream>>>((const double2*)s.zu, s.occ_o, s.norb, s.NL, s.red);
-  k_rho_final<<<(s.NL + 255) / 256, 256, 0, s.stream>>>(s.red, nchunk, s.NL, rho_dev);
+    k_rho_partial<double><<<grid, 256, 0, s.launch_stream()>>>((const double2*)s.zu, s.occ_o, s.norb, s.NL, s.red);
+  k_rho_final<<<(s.NL + 255) / 256, 256, 0, s.launch_stream()>>>(s.red, nchunk, s.NL, rho_dev);
   return cudaGetLastError();
 }
 
@@ -230,19 +230,19 @@ cudaError_t launch_current(System& s, double* jav_dev) {
   cudaError_t e = cudaMemcpyAsync(nab12, h, sizeof(h), cudaMemcpyHostToDevice, s.stream);
   if (e != cudaSuccess) return e;
   if (s.prec == SGPU_PREC_C64) {
-    k_current_orb<float><<<s.norb, 256, 0, s.stream>>>((const float2*)s.zu, s.NLx, s.NLy, s.NLz, nab12, orb);
+    k_current_orb<float><<<s.norb, 256, 0, s.launch_stream()>>>((const float2*)s.zu, s.NLx, s.NLy, s.NLz, nab12, orb);
     if (s.Nlma)
-      k_uvpsi_w<float><<<s.norb, 256, 0, s.stream>>>((const float2*)s.zu, s.NL, s.NBocc, s.zproj64, s.Nlma, s.Nps,
+      k_uvpsi_w<float><<<s.norb, 256, 0, s.launch_stream()>>>((const float2*)s.zu, s.NL, s.NBocc, s.zproj64, s.Nlma, s.Nps,
                                                      s.idx_proj, s.atom_off, s.rpos, s.items, s.nitems, s.lma_list,
                                                      s.Uw);
   } else {
-    k_current_orb<double><<<s.norb, 256, 0, s.stream>>>((const double2*)s.zu, s.NLx, s.NLy, s.NLz, nab12, orb);
+    k_current_orb<double><<<s.norb, 256, 0, s.launch_stream()>>>((const double2*)s.zu, s.NLx, s.NLy, s.NLz, nab12, orb);
     if (s.Nlma)
-      k_uvpsi_w<double><<<s.norb, 256, 0, s.stream>>>((const double2*)s.zu, s.NL, s.NBocc, s.zproj64, s.Nlma,
+      k_uvpsi_w<double><<<s.norb, 256, 0, s.launch_stream()>>>((const double2*)s.zu, s.NL, s.NBocc, s.zproj64, s.Nlma,
                                                       s.Nps, s.idx_proj, s.atom_off, s.rpos, s.items, s.nitems,
                                                       s.lma_list, s.Uw);
   }
-  k_current_final<<<1, 256, 0, s.stream>>>(orb, s.Uw, s.occ_o, s.kAc_d, s.iuV_d, s.norb, s.NBocc, s.Nlma, s.Hxyz,
+  k_current_final<<<1, 256, 0, s.launch_stream()>>>(orb, s.Uw, s.occ_o, s.kAc_d, s.iuV_d, s.norb, s.NBocc, s.Nlma, s.Hxyz,
                                            1.0 / s.aLxyz, jav_dev);
   return cudaGetLastError();
 }
@@ -333,9 +333,9 @@ cudaError_t launch_energy(System& s, double* e_dev) {
   cudaError_t err = cudaMemcpyAsync(coef, h, sizeof(h), cudaMemcpyHostToDevice, s.stream);
   if (err != cudaSuccess) return err;
   if (s.prec == SGPU_PREC_C64)
-    k_ekin_orb<float><<<s.norb, 256, 0, s.stream>>>((const float2*)s.zu, s.NLx, s.NLy, s.NLz, s.NBocc, s.kAc_d, coef, orb);
+    k_ekin_orb<float><<<s.norb, 256, 0, s.launch_stream()>>>((const float2*)s.zu, s.NLx, s.NLy, s.NLz, s.NBocc, s.kAc_d, coef, orb);
   else
-    k_ekin_orb<double><<<s.norb, 256, 0, s.stream>>>((const double2*)s.zu, s.NLx, s.NLy, s.NLz, s.NBocc, s.kAc_d, coef,
+    k_ekin_orb<double><<<s.norb, 256, 0, s.launch_stream()>>>((const double2*)s.zu, s.NLx, s.NLy, s.NLz, s.NBocc, s.kAc_d, coef,
                                                      orb);
   err = cudaGetLastError();
   if (err != cudaSuccess) return err;
@@ -344,7 +344,7 @@ cudaError_t launch_energy(System& s, double* e_dev) {
     err = launch_uvpsi(s, s.zu, 0, s.norb, s.NBocc, false);
     if (err != cudaSuccess) return err;
   }
-  k_energy_final<<<1, 256, 0, s.stream>>>(orb, s.U, s.occ_o, s.kAc_d, s.iuV_d, s.norb, s.NBocc, s.Nlma, s.Hxyz, e_dev);
+  k_energy_final<<<1, 256, 0, s.launch_stream()>>>(orb, s.U, s.occ_o, s.kAc_d, s.iuV_d, s.norb, s.NBocc, s.Nlma, s.Hxyz, e_dev);
   return cudaGetLastError();
 }
 

@@ -781,6 +781,10 @@ extern "C" int sgpu_set_param(sgpu_handle h, int param, int value) {
       if (value < 1 || value > s->NLx) return fail(SGPU_ERR_ARG, "sgpu_set_param: nslab must be in 1..NLx");
       s->nslab = value;
       return 0;
+    case SGPU_PARAM_LAUNCHES:
+      if (value != 0) return fail(SGPU_ERR_ARG, "sgpu_set_param: the launch counter can only be reset to 0");
+      s->launches = 0;
+      return 0;
     default:
       return fail(SGPU_ERR_ARG, "sgpu_set_param: unknown parameter");
   }
@@ -790,6 +794,7 @@ extern "C" int sgpu_get_param(sgpu_handle h, int param, int* value) {
   if (!valid(h) || !value) return fail(SGPU_ERR_ARG, "sgpu_get_param: null argument");
   switch (param) {
     case SGPU_PARAM_NSLAB: *value = h->nslab; return 0;
+    case SGPU_PARAM_LAUNCHES: *value = (int)(h->launches & 0x7fffffffULL); return 0;
     default: return fail(SGPU_ERR_ARG, "sgpu_get_param: unknown parameter");
   }
 }

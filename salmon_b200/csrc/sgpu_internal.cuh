@@ -66,6 +66,13 @@ __device__ __forceinline__ void block_allsum(double (&v)[NV], double* sh) {
 struct System {
   int dev = 0;
   cudaStream_t stream = nullptr;
+  // Kernels launched on `stream` so far (read through SGPU_PARAM_LAUNCHES).
+  mutable unsigned long long launches = 0;
+  // The stream for one kernel launch; counts the launch.
+  cudaStream_t launch_stream() const {
+    ++launches;
+    return stream;
+  }
   int prec = SGPU_PREC_C128;
 
   int NLx = 0, NLy = 0, NLz = 0, NL = 0;
