@@ -11,128 +11,202 @@ namespace sgpu {
 
 // ----------------------------------------------------------------- uVpsi ---
 // U[b][ilma] = Hxyz (iuV) sum_j conj(zproj(j,ilma,k)) in_b(J(j))  (hpsi.f90:188-193)
-// Grid: (orbital pairs, projector items); an item is one atom with <= 4 of its
-// projectors.  The 4 warps of a CTA split the atom's sphere points, accumulate
-// in FP64, reduce by warp shuffles and then across warps in a fixed order
-// (deterministic).  The projectors are read in FP64 for either orbital precision.
-constexpr int UB = 2;
-constexpr int UV_WARPS = 4;
+//
+// A batched dense contraction on the FP64 tensor pipe (mma.sync m8n8k4 f64).
+// For one k-point and one projector item (an atom with <= 4 projectors) the
+// complex contraction over the atom's points j is the real product
+//     C[8][2nb] = A[8][K] B[K][2nb],
+//     A rows 0-3 = Re zproj(j, p), rows 4-7 = Im zproj(j, p)      (p = item projector)
+//     B cols 2b, 2b+1 = Re, Im in_b(J(j))
+// from which U_re[p][b] = C[p][2b] + C[p+4][2b+1] and U_im[p][b] = C[p][2b+1] - C[p+4][2b].
+// Each warp owns one 8x8 tile of C: 4 bands of one k-point ("band quad"),
+// and runs the whole K = Mps of the atom, 4 points per MMA.  Orbital values
+// are converted to FP64 before the MMA, so the contraction is FP64 for either
+// orbital precision, and the summation order is fixed (deterministic).
+constexpr int UM_WARPS = 4;   // band quads per CTA
+constexpr int UM_UNROLL = 16; // MMAs (of 4 points) per batch of loads: 64 points
+
+__device__ __forceinline__ void mma_f64_8x8x4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
 
 template <typename R>
-__global__ void __launch_bounds__(32 * UV_WARPS) k_uvpsi(const C2<R>* __restrict__ in, int nb, int NL, int o_beg,
-                                                        int nbk, const double2* __restrict__ zproj, int Nlma, int Nps,
-                                                        const int* __restrict__ idx_proj, const int* __restrict__ atom_off,
+__global__ void __launch_bounds__(32 * UM_WARPS) k_uvpsi(const C2<R>* __restrict__ in, int ld_in, int o_beg, int nb,
+                                                        int nbk, int kl0, int nquad_k, int nquad,
+                                                        const double2* __restrict__ zproj, int Nlma, int Nps,
+                                                        const int* __restrict__ idx, const int* __restrict__ atom_off,
                                                         const int4* __restrict__ items, const int* __restrict__ lma_list,
                                                         const int* __restrict__ iuV, double scale, int use_iuv,
                                                         double2* __restrict__ U) {
-  __shared__ double2 red[UV_WARPS][4][UB];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int b0 = blockIdx.x * UB;
+  const int quad = blockIdx.x * UM_WARPS + warp;
+  if (quad >= nquad) return;  // whole warp leaves; no block-wide synchronisation follows
+  const int kq = quad / nquad_k;
+  const int kl = kl0 + kq;
+  const int b_first = kl * nbk + 4 * (quad - kq * nquad_k);  // absolute orbital of the quad's first band
+  const int o_lo = max(o_beg, kl * nbk), o_hi = min(o_beg + nb, (kl + 1) * nbk);
   const int4 item = items[blockIdx.y];
   const int a = item.x, l0 = item.y, np = item.z;
   const int p0 = atom_off[a], mps = atom_off[a + 1] - p0;
-  int kl[UB];
-  bool valid[UB];
+
+  // this lane's B element: row (point) lane%4, column n = lane/4 -> band n/2, part n%2
+  const int krow = lane & 3, n = lane >> 2;
+  const int ob = b_first + (n >> 1);
+  const bool bvalid = ob >= o_lo && ob < o_hi;
+  const C2<R>* src = in + (size_t)(bvalid ? ob - o_beg : 0) * ld_in;
+  const int bpart = n & 1;
+  // this lane's A element: row r = lane/4 -> projector r%4, part r/4; column (point) lane%4
+  const int pa = n & 3;
+  const bool avalid = pa < np;
+  const double* zrow =
+      reinterpret_cast<const double*>(zproj + ((size_t)kl * Nlma + (avalid ? lma_list[l0 + pa] : 0)) * Nps) + (n >> 2);
+
+  double c0 = 0.0, c1 = 0.0, e0 = 0.0, e1 = 0.0;  // two accumulator tiles (even / odd MMAs)
+  constexpr int PTS = 4 * UM_UNROLL;              // points per batch; lane l indexes points l and l+32
+  int gl0 = lane < mps ? __ldg(idx + p0 + lane) : 0;
+  int gl1 = 32 + lane < mps ? __ldg(idx + p0 + 32 + lane) : 0;
+  for (int j0 = 0; j0 < mps; j0 += PTS) {
+    // the next batch's point indices are loaded one batch ahead
+    const int jn = j0 + PTS;
+    const int nl0 = jn + lane < mps ? __ldg(idx + p0 + jn + lane) : 0;
+    const int nl1 = jn + 32 + lane < mps ? __ldg(idx + p0 + jn + 32 + lane) : 0;
+    double av[UM_UNROLL], bv[UM_UNROLL];
 #pragma unroll
-  for (int u = 0; u < UB; ++u) {
-    valid[u] = (b0 + u) < nb;
-    kl[u] = valid[u] ? (o_beg + b0 + u) / nbk : 0;
-  }
-  bool samek = true;
-#pragma unroll
-  for (int u = 1; u < UB; ++u) samek = samek && (!valid[u] || kl[u] == kl[0]);
-  int ilma[4];
-#pragma unroll
-  for (int p = 0; p < 4; ++p) ilma[p] = p < np ? lma_list[l0 + p] : 0;
-  double2 acc[4][UB];
-#pragma unroll
-  for (int p = 0; p < 4; ++p)
-#pragma unroll
-    for (int u = 0; u < UB; ++u) acc[p][u] = make_double2(0, 0);
-#pragma unroll 4
-  for (int j = threadIdx.x; j < mps; j += 32 * UV_WARPS) {
-    const int gi = __ldg(idx_proj + p0 + j);
-    double2 v[UB];
-#pragma unroll
-    for (int u = 0; u < UB; ++u) v[u] = valid[u] ? to_d2(in[(size_t)(b0 + u) * NL + gi]) : make_double2(0, 0);
-#pragma unroll
-    for (int p = 0; p < 4; ++p) {
-      if (p < np) {
-        if (samek) {
-          const double2 z = __ldg(zproj + ((size_t)kl[0] * Nlma + ilma[p]) * Nps + j);
-#pragma unroll
-          for (int u = 0; u < UB; ++u) acc[p][u] = cfmaj(z, v[u], acc[p][u]);
-        } else {
-#pragma unroll
-          for (int u = 0; u < UB; ++u) {
-            const double2 z = __ldg(zproj + ((size_t)kl[u] * Nlma + ilma[p]) * Nps + j);
-            acc[p][u] = cfmaj(z, v[u], acc[p][u]);
-          }
+    for (int u = 0; u < UM_UNROLL; ++u) {
+      const int j = j0 + 4 * u + krow;
+      const int g = __shfl_sync(0xffffffffu, u < UM_UNROLL / 2 ? gl0 : gl1, (4 * u + krow) & 31);
+      av[u] = 0.0;
+      bv[u] = 0.0;
+      if (j < mps) {
+        if (avalid) av[u] = __ldg(zrow + 2 * (size_t)j);
+        if (bvalid) {
+          const C2<R> v = src[g];
+          bv[u] = bpart ? (double)v.y : (double)v.x;
         }
       }
     }
-  }
 #pragma unroll
-  for (int p = 0; p < 4; ++p)
-#pragma unroll
-    for (int u = 0; u < UB; ++u) {
-      double2 s = acc[p][u];
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        s.x += __shfl_xor_sync(0xffffffffu, s.x, off);
-        s.y += __shfl_xor_sync(0xffffffffu, s.y, off);
-      }
-      if (lane == 0) red[warp][p][u] = s;
+    for (int u = 0; u < UM_UNROLL; u += 2) {
+      mma_f64_8x8x4(c0, c1, av[u], bv[u]);
+      mma_f64_8x8x4(e0, e1, av[u + 1], bv[u + 1]);
     }
-  __syncthreads();
-  if (threadIdx.x < 4 * UB) {
-    const int p = threadIdx.x / UB, u = threadIdx.x % UB;
-    if (p < np && valid[u]) {
-      double2 s = red[0][p][u];
-#pragma unroll
-      for (int w = 1; w < UV_WARPS; ++w) {
-        s.x += red[w][p][u].x;
-        s.y += red[w][p][u].y;
-      }
-      const double f = scale * (use_iuv ? (double)iuV[ilma[p]] : 1.0);
-      U[(size_t)(b0 + u) * Nlma + ilma[p]] = make_double2(s.x * f, s.y * f);
+    gl0 = nl0;
+    gl1 = nl1;
+  }
+  c0 += e0;
+  c1 += e1;
+  // lane holds C[r = lane/4][2*(lane%4) + i]; the Im-zproj rows r+4 sit 16 lanes up
+  const double d0 = __shfl_down_sync(0xffffffffu, c0, 16);
+  const double d1 = __shfl_down_sync(0xffffffffu, c1, 16);
+  if (lane < 16) {
+    const int p = lane >> 2, o = b_first + (lane & 3);
+    if (p < np && o >= o_lo && o < o_hi) {
+      const int ilma = lma_list[l0 + p];
+      const double f = scale * (use_iuv ? (double)iuV[ilma] : 1.0);
+      U[(size_t)(o - o_beg) * Nlma + ilma] = make_double2((c0 + d1) * f, (c1 - d0) * f);
     }
   }
+}
+
+template <typename R>
+static cudaError_t launch_uvpsi_t(const System& s, const void* in, int ld_in, const int* idx, int o_beg, int nb,
+                                  int nbk, bool scale_iuv) {
+  const int kl0 = o_beg / nbk, kl1 = (o_beg + nb - 1) / nbk;
+  const int nquad_k = (nbk + 3) / 4;
+  const int nquad = (kl1 - kl0 + 1) * nquad_k;
+  dim3 grid((nquad + UM_WARPS - 1) / UM_WARPS, s.nitems);
+  k_uvpsi<R><<<grid, 32 * UM_WARPS, 0, s.launch_stream()>>>((const C2<R>*)in, ld_in, o_beg, nb, nbk, kl0, nquad_k,
+                                                             nquad, s.zproj64, s.Nlma, s.Nps, idx, s.atom_off, s.items,
+                                                             s.lma_list, s.iuV_d, s.Hxyz, scale_iuv ? 1 : 0, s.U);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_uvpsi(const System& s, const void* in, int o_beg, int nb, int nbk, bool scale_iuv, int prec) {
   if (s.Nlma == 0 || nb == 0) return cudaSuccess;
-  dim3 grid((nb + UB - 1) / UB, s.nitems);
   if ((prec < 0 ? s.prec : prec) == SGPU_PREC_C64)
-    k_uvpsi<float><<<grid, 32 * UV_WARPS, 0, s.launch_stream()>>>((const float2*)in, nb, s.NL, o_beg, nbk, s.zproj64, s.Nlma,
-                                                         s.Nps, s.idx_proj, s.atom_off, s.items, s.lma_list, s.iuV_d,
-                                                         s.Hxyz, scale_iuv ? 1 : 0, s.U);
-  else
-    k_uvpsi<double><<<grid, 32 * UV_WARPS, 0, s.launch_stream()>>>((const double2*)in, nb, s.NL, o_beg, nbk, s.zproj64, s.Nlma,
-                                                          s.Nps, s.idx_proj, s.atom_off, s.items, s.lma_list, s.iuV_d,
-                                                          s.Hxyz, scale_iuv ? 1 : 0, s.U);
-  return cudaGetLastError();
+    return launch_uvpsi_t<float>(s, in, s.NL, s.idx_proj, o_beg, nb, nbk, scale_iuv);
+  return launch_uvpsi_t<double>(s, in, s.NL, s.idx_proj, o_beg, nb, nbk, scale_iuv);
 }
 
 cudaError_t launch_uvpsi_from_S(const System& s, const void* S, int o_beg, int nb, int nbk, bool scale_iuv) {
   if (s.Nlma == 0 || nb == 0) return cudaSuccess;
-  dim3 grid((nb + UB - 1) / UB, s.nitems);
-  if (s.prec == SGPU_PREC_C64)
-    k_uvpsi<float><<<grid, 32 * UV_WARPS, 0, s.launch_stream()>>>((const float2*)S, nb, s.nsp, o_beg, nbk, s.zproj64, s.Nlma,
-                                                         s.Nps, s.qmap, s.atom_off, s.items, s.lma_list, s.iuV_d,
-                                                         s.Hxyz, scale_iuv ? 1 : 0, s.U);
-  else
-    k_uvpsi<double><<<grid, 32 * UV_WARPS, 0, s.launch_stream()>>>((const double2*)S, nb, s.nsp, o_beg, nbk, s.zproj64, s.Nlma,
-                                                          s.Nps, s.qmap, s.atom_off, s.items, s.lma_list, s.iuV_d,
-                                                          s.Hxyz, scale_iuv ? 1 : 0, s.U);
-  return cudaGetLastError();
+  if (s.prec == SGPU_PREC_C64) return launch_uvpsi_t<float>(s, S, s.nsp, s.qmap, o_beg, nb, nbk, scale_iuv);
+  return launch_uvpsi_t<double>(s, S, s.nsp, s.qmap, o_beg, nb, nbk, scale_iuv);
 }
 
 // ------------------------------------------------------------- KB field ---
 // W[b][q] = sum over the (ilma, j) entries of sphere point q of zproj(j,ilma,k) U[b][ilma]
-// (the dpseudo of pseudo_pt, common/hpsi.f90:194-200, already summed per grid
-// point), in entry order.  One thread per sphere point and KU orbitals; a
-// zproj value is loaded once for orbitals on the same k-point.
+// (the dpseudo of pseudo_pt, common/hpsi.f90:194-200, summed per grid point).
+//
+// Points inside exactly one projector item (the usual case: non-overlapping
+// spheres, <= 4 projectors per atom) go through the FP64 tensor pipe: for one
+// k-point, item and band quad the field at 8 points is the real product
+//     C[8][8] = A[8][8] B[8][8],
+//     A[m][p] = Re zproj(j_m, p), A[m][4+p] = Im zproj(j_m, p),
+//     B[p][2b] = Re U[b][p], B[p][2b+1] = Im U[b][p], B[4+p][2b] = -Im U[b][p], B[4+p][2b+1] = Re U[b][p],
+// two m8n8k4 MMAs per tile of 8 points; B stays in registers for the warp's
+// whole sweep over the atom.  Points that lie in several items are summed
+// entry by entry in a fixed order by k_kbfield_multi, so every W element has
+// one writer and the result is deterministic.
+template <typename R>
+__global__ void __launch_bounds__(32 * UM_WARPS) k_kbfield(const double2* __restrict__ U, int o_beg, int nb, int nbk,
+                                                          int kl0, int nquad_k, int nquad,
+                                                          const double2* __restrict__ zproj, int Nlma, int Nps,
+                                                          const int* __restrict__ kbq, const int* __restrict__ atom_off,
+                                                          const int4* __restrict__ items,
+                                                          const int* __restrict__ lma_list, int nsp,
+                                                          C2<R>* __restrict__ W) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int quad = blockIdx.x * UM_WARPS + warp;
+  if (quad >= nquad) return;  // whole warp leaves; no block-wide synchronisation follows
+  const int kq = quad / nquad_k;
+  const int kl = kl0 + kq;
+  const int b_first = kl * nbk + 4 * (quad - kq * nquad_k);
+  const int o_lo = max(o_beg, kl * nbk), o_hi = min(o_beg + nb, (kl + 1) * nbk);
+  const int4 item = items[blockIdx.y];
+  const int a = item.x, l0 = item.y, np = item.z;
+  const int p0 = atom_off[a], mps = atom_off[a + 1] - p0;
+
+  // B fragment (row p = lane%4, column n = lane/4 -> band n/2, part n%2): constant
+  const int p = lane & 3, n = lane >> 2;
+  const int ob = b_first + (n >> 1);
+  double2 u = make_double2(0.0, 0.0);
+  if (p < np && ob >= o_lo && ob < o_hi) u = U[(size_t)(ob - o_beg) * Nlma + lma_list[l0 + p]];
+  const double bre = (n & 1) ? u.y : u.x;   // rows of Re zproj
+  const double bim = (n & 1) ? u.x : -u.y;  // rows of Im zproj
+  // A fragment (row m = lane/4 -> point, column p = lane%4); C: row m, columns 2*(lane%4)+{0,1}
+  const double2* zp = zproj + ((size_t)kl * Nlma + (p < np ? lma_list[l0 + p] : 0)) * Nps;
+  const int oc = b_first + p;  // the orbital of this lane's C elements
+  const bool cvalid = oc >= o_lo && oc < o_hi;
+  C2<R>* Wb = W + (size_t)(cvalid ? oc - o_beg : 0) * nsp;
+  constexpr int T = 8;  // tiles of 8 points per batch of loads
+  for (int j0 = 0; j0 < mps; j0 += 8 * T) {
+    double2 z[T];
+    int q[T];
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+      const int j = j0 + 8 * t + n;
+      z[t] = make_double2(0.0, 0.0);
+      q[t] = -1;
+      if (j < mps) {
+        if (p < np) z[t] = __ldg(zp + j);
+        q[t] = __ldg(kbq + p0 + j);
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+      double c0 = 0.0, c1 = 0.0;
+      mma_f64_8x8x4(c0, c1, z[t].x, bre);
+      mma_f64_8x8x4(c0, c1, z[t].y, bim);
+      if (cvalid && q[t] >= 0) Wb[q[t]] = mk<R>((R)c0, (R)c1);
+    }
+  }
+}
+
+// Points in several projector items: one thread per (listed point, orbital
+// group), entries summed in their table order.
 constexpr int KU = 4;
 
 __device__ __forceinline__ int kb_entry(const int4& ra, const int4& rb, const int* cont, int e) {
@@ -141,55 +215,54 @@ __device__ __forceinline__ int kb_entry(const int4& ra, const int4& rb, const in
 }
 
 template <typename R>
-__global__ void __launch_bounds__(256) k_kbfield(const double2* __restrict__ U, int nb, int o_beg, int nbk,
-                                                 const C2<R>* __restrict__ zproj, int Nlma, int Nps,
-                                                 const int4* __restrict__ rec, const int* __restrict__ cont, int nsp,
-                                                 C2<R>* __restrict__ W) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) k_kbfield_multi(const double2* __restrict__ U, int nb, int o_beg, int nbk,
+                                                       const double2* __restrict__ zproj, int Nlma, int Nps,
+                                                       const int4* __restrict__ rec, const int* __restrict__ cont,
+                                                       const int* __restrict__ qlist, int nq, int nsp,
+                                                       C2<R>* __restrict__ W) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int b0 = blockIdx.y * KU;
-  if (q >= nsp) return;
+  if (t >= nq) return;
+  const int q = qlist[t];
   const int4 ra = __ldg(rec + 2 * (size_t)q), rb = __ldg(rec + 2 * (size_t)q + 1);
   const int ne = ra.y + rb.w;
-  int kl[KU];
-  bool valid[KU];
 #pragma unroll
   for (int u = 0; u < KU; ++u) {
-    valid[u] = b0 + u < nb;
-    kl[u] = valid[u] ? (o_beg + b0 + u) / nbk : 0;
-  }
-  bool samek = true;
-#pragma unroll
-  for (int u = 1; u < KU; ++u) samek = samek && (!valid[u] || kl[u] == kl[0]);
-  C2<R> acc[KU];
-#pragma unroll
-  for (int u = 0; u < KU; ++u) acc[u] = mk<R>(0, 0);
-  for (int e = 0; e < ne; ++e) {
-    const int en = kb_entry(ra, rb, cont, e);
-    const int ilma = en >> 16, zoff = ilma * Nps + (en & 0xffff);
-    C2<R> z0 = __ldg(zproj + (size_t)kl[0] * Nlma * Nps + zoff);
-#pragma unroll
-    for (int u = 0; u < KU; ++u) {
-      if (!valid[u]) continue;
-      const C2<R> z = samek ? z0 : __ldg(zproj + (size_t)kl[u] * Nlma * Nps + zoff);
+    if (b0 + u >= nb) break;
+    const int kl = (o_beg + b0 + u) / nbk;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int e = 0; e < ne; ++e) {
+      const int en = kb_entry(ra, rb, cont, e);
+      const int ilma = en >> 16;
+      const double2 z = __ldg(zproj + ((size_t)kl * Nlma + ilma) * Nps + (en & 0xffff));
       const double2 uu = __ldg(U + (size_t)(b0 + u) * Nlma + ilma);
-      acc[u] = cfma(z, mk<R>((R)uu.x, (R)uu.y), acc[u]);
+      acc = cfma(z, uu, acc);
     }
+    W[(size_t)(b0 + u) * nsp + q] = mk<R>((R)acc.x, (R)acc.y);
   }
-#pragma unroll
-  for (int u = 0; u < KU; ++u)
-    if (valid[u]) W[(size_t)(b0 + u) * nsp + q] = acc[u];
+}
+
+template <typename R>
+static cudaError_t launch_kbfield_t(const System& s, int o_beg, int nb, int nbk, void* W) {
+  const int kl0 = o_beg / nbk, kl1 = (o_beg + nb - 1) / nbk;
+  const int nquad_k = (nbk + 3) / 4;
+  const int nquad = (kl1 - kl0 + 1) * nquad_k;
+  dim3 grid((nquad + UM_WARPS - 1) / UM_WARPS, s.nitems);
+  k_kbfield<R><<<grid, 32 * UM_WARPS, 0, s.launch_stream()>>>(s.U, o_beg, nb, nbk, kl0, nquad_k, nquad, s.zproj64,
+                                                               s.Nlma, s.Nps, s.kbq, s.atom_off, s.items, s.lma_list,
+                                                               s.nsp, (C2<R>*)W);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || s.n_multi == 0) return e;
+  dim3 g2((s.n_multi + 255) / 256, (nb + KU - 1) / KU);
+  k_kbfield_multi<R><<<g2, 256, 0, s.launch_stream()>>>(s.U, nb, o_beg, nbk, s.zproj64, s.Nlma, s.Nps, s.rec, s.cont,
+                                                         s.kb_multi, s.n_multi, s.nsp, (C2<R>*)W);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_kbfield(const System& s, int o_beg, int nb, int nbk, void* W, int prec) {
   if (s.nsp == 0 || nb == 0) return cudaSuccess;
-  dim3 grid((s.nsp + 255) / 256, (nb + KU - 1) / KU);
-  if ((prec < 0 ? s.prec : prec) == SGPU_PREC_C64)
-    k_kbfield<float><<<grid, 256, 0, s.launch_stream()>>>(s.U, nb, o_beg, nbk, s.zproj32, s.Nlma, s.Nps, s.rec, s.cont, s.nsp,
-                                                (float2*)W);
-  else
-    k_kbfield<double><<<grid, 256, 0, s.launch_stream()>>>(s.U, nb, o_beg, nbk, s.zproj64, s.Nlma, s.Nps, s.rec, s.cont, s.nsp,
-                                                 (double2*)W);
-  return cudaGetLastError();
+  if ((prec < 0 ? s.prec : prec) == SGPU_PREC_C64) return launch_kbfield_t<float>(s, o_beg, nb, nbk, W);
+  return launch_kbfield_t<double>(s, o_beg, nb, nbk, W);
 }
 
 // ------------------------------------------------------ update_projector ---

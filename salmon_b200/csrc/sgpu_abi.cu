@@ -213,7 +213,7 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
   // packed projector points to sphere points
   std::vector<int> sp_off(s->NLx + 1, 0), q_of(s->NL, -1), qmap(std::max(1, s->NPI), 0);
   std::vector<int4> rec;
-  std::vector<int> cont;
+  std::vector<int> cont, kbq, kb_multi;
   {
     if (s->Nps >= 65536 || s->Nlma >= 32768)
       return bail(fail(SGPU_ERR_UNSUPPORTED, "sgpu_create: Nps must be < 65536 and Nlma < 32768"));
@@ -241,6 +241,15 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
     s->nsp = nsp;
     for (int x = 0; x < s->NLx; ++x) s->maxpts = std::max(s->maxpts, sp_off[x + 1] - sp_off[x]);
     for (int p = 0; p < s->NPI; ++p) qmap[p] = q_of[idx_proj[p]];
+    // items covering each sphere point (an item covers every point of its atom)
+    std::vector<int> icnt(std::max(1, nsp), 0);
+    for (const int4& it : items)
+      for (int p = atom_off[it.x]; p < atom_off[it.x + 1]; ++p) icnt[qmap[p]]++;
+    kbq.resize(std::max(1, s->NPI), -1);
+    for (int p = 0; p < s->NPI; ++p) kbq[p] = icnt[qmap[p]] == 1 ? qmap[p] : -1;
+    for (int q = 0; q < nsp; ++q)
+      if (icnt[q] > 1) kb_multi.push_back(q);
+    s->n_multi = (int)kb_multi.size();
     if (s->maxpts > 32767) return bail(fail(SGPU_ERR_UNSUPPORTED, "sgpu_create: more than 32767 sphere points in one x-plane"));
   }
   std::vector<short> lqi(s->NL, (short)-1);
@@ -274,6 +283,8 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
   UP(s->rec, rec);
   UP(s->cont, cont);
   UP(s->qmap, qmap);
+  UP(s->kbq, kbq);
+  UP(s->kb_multi, kb_multi);
   UP(s->lqi, lqi);
   UP(s->occ_o, occo);
 #undef UP
@@ -320,7 +331,7 @@ int sgpu_destroy(sgpu_handle h) {
   if (s->stream) cudaStreamSynchronize(s->stream);
   free_state_buffers(s);
   void* bufs[] = {s->vloc64, s->vloc32, s->occ_o, s->kAc_d, s->idx_proj, s->atom_off, s->rpos, s->items,
-                  s->lma_list, s->iuV_d, s->lma_atom, s->uV_d, s->zproj64, s->zproj32, s->sp_off, s->rec, s->cont, s->qmap, s->lqi, s->Sbuf, s->Wbuf,
+                  s->lma_list, s->iuV_d, s->lma_atom, s->uV_d, s->zproj64, s->zproj32, s->sp_off, s->rec, s->cont, s->qmap, s->kbq, s->kb_multi, s->lqi, s->Sbuf, s->Wbuf,
                   s->U, s->Uw, s->red, s->stage};
   for (void* p : bufs) cudaFree(p);
   void* gbufs[] = {s->gs_zu, s->gs_aux, s->gs_W, s->gs_st, s->gs_part, s->gs_A, s->gs_V, s->gs_w, s->gs_sweeps,

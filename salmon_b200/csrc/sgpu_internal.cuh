@@ -117,6 +117,12 @@ struct System {
   int4* rec = nullptr;             // [2*nsp]
   int* cont = nullptr;             // entries beyond the 4th of points in several spheres
   int* qmap = nullptr;             // [NPI]
+  // KB field on the tensor pipe: kbq[p] = qmap[p] where the sphere point lies in
+  // exactly one projector item, else -1; those other points (kb_multi, n_multi
+  // of them) are summed entry by entry in a fixed order instead.
+  int* kbq = nullptr;              // [NPI]
+  int* kb_multi = nullptr;         // [n_multi]
+  int n_multi = 0;
   short* lqi = nullptr;            // [NL]
   int nsp = 0, maxpts = 0;
   void* Wbuf = nullptr;            // [W_rows][nsp] KB field (element: complex(8) capacity)
