@@ -19,12 +19,14 @@ namespace sgpu {
 //     A rows 0-3 = Re zproj(j, p), rows 4-7 = Im zproj(j, p)      (p = item projector)
 //     B cols 2b, 2b+1 = Re, Im in_b(J(j))
 // from which U_re[p][b] = C[p][2b] + C[p+4][2b+1] and U_im[p][b] = C[p][2b+1] - C[p+4][2b].
-// Each warp owns one 8x8 tile of C: 4 bands of one k-point ("band quad"),
-// and runs the whole K = Mps of the atom, 4 points per MMA.  Orbital values
-// are converted to FP64 before the MMA, so the contraction is FP64 for either
-// orbital precision, and the summation order is fixed (deterministic).
-constexpr int UM_WARPS = 4;   // band quads per CTA
-constexpr int UM_UNROLL = 16; // MMAs (of 4 points) per batch of loads: 64 points
+// A CTA owns one 8x8 tile of C: 4 bands of one k-point ("band quad") and one
+// item; its UM_SPLIT warps split K (the atom's points, in chunks of 32) and
+// their tiles are added in warp order, so the sum order is fixed
+// (deterministic).  Orbital values are converted to FP64 before the MMA: the
+// contraction is FP64 for either orbital precision.
+constexpr int UM_WARPS = 4;   // band quads per CTA (KB field)
+constexpr int UM_SPLIT = 4;   // warps splitting the points of one (quad, item) (projections)
+constexpr int UM_UNROLL = 8;  // MMAs (of 4 points) per batch of loads: 32 points
 
 __device__ __forceinline__ void mma_f64_8x8x4(double& d0, double& d1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
@@ -33,16 +35,16 @@ __device__ __forceinline__ void mma_f64_8x8x4(double& d0, double& d1, double a, 
 }
 
 template <typename R>
-__global__ void __launch_bounds__(32 * UM_WARPS) k_uvpsi(const C2<R>* __restrict__ in, int ld_in, int o_beg, int nb,
-                                                        int nbk, int kl0, int nquad_k, int nquad,
+__global__ void __launch_bounds__(32 * UM_SPLIT) k_uvpsi(const C2<R>* __restrict__ in, int ld_in, int o_beg, int nb,
+                                                        int nbk, int kl0, int nquad_k,
                                                         const double2* __restrict__ zproj, int Nlma, int Nps,
                                                         const int* __restrict__ idx, const int* __restrict__ atom_off,
                                                         const int4* __restrict__ items, const int* __restrict__ lma_list,
                                                         const int* __restrict__ iuV, double scale, int use_iuv,
                                                         double2* __restrict__ U) {
+  __shared__ double2 part[UM_SPLIT][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int quad = blockIdx.x * UM_WARPS + warp;
-  if (quad >= nquad) return;  // whole warp leaves; no block-wide synchronisation follows
+  const int quad = blockIdx.x;
   const int kq = quad / nquad_k;
   const int kl = kl0 + kq;
   const int b_first = kl * nbk + 4 * (quad - kq * nquad_k);  // absolute orbital of the quad's first band
@@ -64,19 +66,19 @@ __global__ void __launch_bounds__(32 * UM_WARPS) k_uvpsi(const C2<R>* __restrict
       reinterpret_cast<const double*>(zproj + ((size_t)kl * Nlma + (avalid ? lma_list[l0 + pa] : 0)) * Nps) + (n >> 2);
 
   double c0 = 0.0, c1 = 0.0, e0 = 0.0, e1 = 0.0;  // two accumulator tiles (even / odd MMAs)
-  constexpr int PTS = 4 * UM_UNROLL;              // points per batch; lane l indexes points l and l+32
-  int gl0 = lane < mps ? __ldg(idx + p0 + lane) : 0;
-  int gl1 = 32 + lane < mps ? __ldg(idx + p0 + 32 + lane) : 0;
-  for (int j0 = 0; j0 < mps; j0 += PTS) {
-    // the next batch's point indices are loaded one batch ahead
-    const int jn = j0 + PTS;
-    const int nl0 = jn + lane < mps ? __ldg(idx + p0 + jn + lane) : 0;
-    const int nl1 = jn + 32 + lane < mps ? __ldg(idx + p0 + jn + 32 + lane) : 0;
+  constexpr int PTS = 4 * UM_UNROLL;              // points per chunk (one per lane for the index load)
+  constexpr int STRIDE = PTS * UM_SPLIT;
+  int j0 = warp * PTS;
+  int gl = j0 + lane < mps ? __ldg(idx + p0 + j0 + lane) : 0;
+  for (; j0 < mps; j0 += STRIDE) {
+    // the next chunk's point indices are loaded one chunk ahead
+    const int jn = j0 + STRIDE;
+    const int nl = jn + lane < mps ? __ldg(idx + p0 + jn + lane) : 0;
     double av[UM_UNROLL], bv[UM_UNROLL];
 #pragma unroll
     for (int u = 0; u < UM_UNROLL; ++u) {
       const int j = j0 + 4 * u + krow;
-      const int g = __shfl_sync(0xffffffffu, u < UM_UNROLL / 2 ? gl0 : gl1, (4 * u + krow) & 31);
+      const int g = __shfl_sync(0xffffffffu, gl, 4 * u + krow);
       av[u] = 0.0;
       bv[u] = 0.0;
       if (j < mps) {
@@ -92,20 +94,27 @@ __global__ void __launch_bounds__(32 * UM_WARPS) k_uvpsi(const C2<R>* __restrict
       mma_f64_8x8x4(c0, c1, av[u], bv[u]);
       mma_f64_8x8x4(e0, e1, av[u + 1], bv[u + 1]);
     }
-    gl0 = nl0;
-    gl1 = nl1;
+    gl = nl;
   }
-  c0 += e0;
-  c1 += e1;
-  // lane holds C[r = lane/4][2*(lane%4) + i]; the Im-zproj rows r+4 sit 16 lanes up
-  const double d0 = __shfl_down_sync(0xffffffffu, c0, 16);
-  const double d1 = __shfl_down_sync(0xffffffffu, c1, 16);
-  if (lane < 16) {
-    const int p = lane >> 2, o = b_first + (lane & 3);
-    if (p < np && o >= o_lo && o < o_hi) {
-      const int ilma = lma_list[l0 + p];
-      const double f = scale * (use_iuv ? (double)iuV[ilma] : 1.0);
-      U[(size_t)(o - o_beg) * Nlma + ilma] = make_double2((c0 + d1) * f, (c1 - d0) * f);
+  part[warp][lane] = make_double2(c0 + e0, c1 + e1);
+  __syncthreads();
+  if (warp == 0) {
+    double2 t = part[0][lane];
+#pragma unroll
+    for (int w = 1; w < UM_SPLIT; ++w) {
+      t.x += part[w][lane].x;
+      t.y += part[w][lane].y;
+    }
+    // lane holds C[r = lane/4][2*(lane%4) + i]; the Im-zproj rows r+4 sit 16 lanes up
+    const double d0 = __shfl_down_sync(0xffffffffu, t.x, 16);
+    const double d1 = __shfl_down_sync(0xffffffffu, t.y, 16);
+    if (lane < 16) {
+      const int p = lane >> 2, o = b_first + (lane & 3);
+      if (p < np && o >= o_lo && o < o_hi) {
+        const int ilma = lma_list[l0 + p];
+        const double f = scale * (use_iuv ? (double)iuV[ilma] : 1.0);
+        U[(size_t)(o - o_beg) * Nlma + ilma] = make_double2((t.x + d1) * f, (t.y - d0) * f);
+      }
     }
   }
 }
@@ -116,9 +125,9 @@ static cudaError_t launch_uvpsi_t(const System& s, const void* in, int ld_in, co
   const int kl0 = o_beg / nbk, kl1 = (o_beg + nb - 1) / nbk;
   const int nquad_k = (nbk + 3) / 4;
   const int nquad = (kl1 - kl0 + 1) * nquad_k;
-  dim3 grid((nquad + UM_WARPS - 1) / UM_WARPS, s.nitems);
-  k_uvpsi<R><<<grid, 32 * UM_WARPS, 0, s.launch_stream()>>>((const C2<R>*)in, ld_in, o_beg, nb, nbk, kl0, nquad_k,
-                                                             nquad, s.zproj64, s.Nlma, s.Nps, idx, s.atom_off, s.items,
+  dim3 grid(nquad, s.nitems);
+  k_uvpsi<R><<<grid, 32 * UM_SPLIT, 0, s.launch_stream()>>>((const C2<R>*)in, ld_in, o_beg, nb, nbk, kl0, nquad_k,
+                                                             s.zproj64, s.Nlma, s.Nps, idx, s.atom_off, s.items,
                                                              s.lma_list, s.iuV_d, s.Hxyz, scale_iuv ? 1 : 0, s.U);
   return cudaGetLastError();
 }
