@@ -239,8 +239,9 @@ int sgpu_gs_to_rt(sgpu_handle h);
 
 /* ---- tuning --------------------------------------------------------------- */
 enum {
-  SGPU_PARAM_NSLAB = 0,   /* CTAs per orbital along x in the stencil pass (1..NLx) */
-  SGPU_PARAM_LAUNCHES = 1 /* kernels the handle has launched, modulo 2^31 (read; set to 0 to reset) */
+  SGPU_PARAM_NSLAB = 0,       /* CTAs per orbital along x in the stencil pass (1..NLx)              */
+  SGPU_PARAM_LAUNCHES = 1,    /* kernels the handle has launched, modulo 2^31 (read; set 0 to reset) */
+  SGPU_PARAM_UVPSI_SPLIT = 2  /* warps splitting the points of one projection tile: 1, 2, 4 or 8     */
 };
 
 /* Sets / reads a launch parameter of the handle (the autotuner's knobs).  No
@@ -248,6 +249,35 @@ enum {
  * (modules/opt_variables.f90:340-353), which picks cache blocking sizes. */
 int sgpu_set_param(sgpu_handle h, int param, int value);
 int sgpu_get_param(sgpu_handle h, int param, int* value);
+
+/* Autotuner: times `reps` H applications of the resident orbitals (projections,
+ * KB field, stencil pass) for every launch shape it knows (x-slabs per orbital
+ * 1, 2, 4; projection split 1, 2, 4, 8), keeps the fastest in the handle and
+ * returns it (any output pointer may be NULL).  The resident orbitals are not
+ * modified.  No reference counterpart; the nearest is auto_blocking
+ * (modules/opt_variables.f90:340-353). */
+int sgpu_autotune(sgpu_handle h, int reps, int* nslab, int* split, double* ms_per_apply);
+
+/* ---- batched systems ------------------------------------------------------ */
+/* Several systems (handles on the current device) advanced together.  No
+ * reference counterpart: the reference runs one system per process. */
+typedef struct sgpu_batch* sgpu_batch_handle;
+
+int sgpu_batch_create(const sgpu_handle* handles, int n, sgpu_batch_handle* out);
+
+/* nsteps Taylor steps of every system, system i with time step dt[i] (HOST,
+ * n values), each with the Hamiltonian of its last sgpu_update_projector /
+ * sgpu_set_vloc.  The steps of all systems are captured once into a CUDA graph
+ * (each system on its own stream) and replayed on later calls with the same
+ * dt[] and nsteps; a call with other values, or after a handle's precision
+ * changed, captures again (and first waits for the handles' queued work).
+ * Asynchronous: later calls on a handle are ordered after the replay. */
+int sgpu_batch_step(sgpu_batch_handle b, const double* dt, int nsteps);
+
+/* The batch's cudaStream_t (the replay runs on it). */
+void* sgpu_batch_stream(sgpu_batch_handle b);
+
+int sgpu_batch_destroy(sgpu_batch_handle b);
 
 /* ---- instrumentation ----------------------------------------------------- */
 /* Kernels that sgpu_time_kernel can time. */

@@ -44,9 +44,14 @@ ABI = {
     "sgpu_gs_to_rt": (C.c_int, [_vp]),
     "sgpu_set_param": (C.c_int, [_vp, _ip, _ip]),
     "sgpu_get_param": (C.c_int, [_vp, _ip, C.POINTER(C.c_int)]),
+    "sgpu_autotune": (C.c_int, [_vp, _ip, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]),
+    "sgpu_batch_create": (C.c_int, [C.POINTER(C.c_void_p), _ip, C.POINTER(C.c_void_p)]),
+    "sgpu_batch_step": (C.c_int, [_vp, _vp, _ip]),
+    "sgpu_batch_stream": (C.c_void_p, [_vp]),
+    "sgpu_batch_destroy": (C.c_int, [_vp]),
 }
 
-PARAMS = {"nslab": 0, "launches": 1}
+PARAMS = {"nslab": 0, "launches": 1, "uvpsi_split": 2}
 
 KERNELS = {"stencil_pass": 0, "taylor_last": 1, "uvpsi": 2, "psi_rho": 3, "kb_field": 4}
 

@@ -20,12 +20,12 @@ namespace sgpu {
 //     B cols 2b, 2b+1 = Re, Im in_b(J(j))
 // from which U_re[p][b] = C[p][2b] + C[p+4][2b+1] and U_im[p][b] = C[p][2b+1] - C[p+4][2b].
 // A CTA owns one 8x8 tile of C: 4 bands of one k-point ("band quad") and one
-// item; its UM_SPLIT warps split K (the atom's points, in chunks of 32) and
+// item; its UM_SPLIT warps (a tuning parameter: 1, 2, 4 or 8) split K (the
+// atom's points, in chunks of 32) and
 // their tiles are added in warp order, so the sum order is fixed
 // (deterministic).  Orbital values are converted to FP64 before the MMA: the
 // contraction is FP64 for either orbital precision.
 constexpr int UM_WARPS = 4;   // band quads per CTA (KB field)
-constexpr int UM_SPLIT = 4;   // warps splitting the points of one (quad, item) (projections)
 constexpr int UM_UNROLL = 8;  // MMAs (of 4 points) per batch of loads: 32 points
 
 __device__ __forceinline__ void mma_f64_8x8x4(double& d0, double& d1, double a, double b) {
@@ -34,7 +34,7 @@ __device__ __forceinline__ void mma_f64_8x8x4(double& d0, double& d1, double a, 
                : "d"(a), "d"(b));
 }
 
-template <typename R>
+template <typename R, int UM_SPLIT>
 __global__ void __launch_bounds__(32 * UM_SPLIT) k_uvpsi(const C2<R>* __restrict__ in, int ld_in, int o_beg, int nb,
                                                         int nbk, int kl0, int nquad_k,
                                                         const double2* __restrict__ zproj, int Nlma, int Nps,
@@ -119,17 +119,28 @@ __global__ void __launch_bounds__(32 * UM_SPLIT) k_uvpsi(const C2<R>* __restrict
   }
 }
 
-template <typename R>
-static cudaError_t launch_uvpsi_t(const System& s, const void* in, int ld_in, const int* idx, int o_beg, int nb,
-                                  int nbk, bool scale_iuv) {
+template <typename R, int SPLIT>
+static cudaError_t launch_uvpsi_split(const System& s, const void* in, int ld_in, const int* idx, int o_beg, int nb,
+                                      int nbk, bool scale_iuv) {
   const int kl0 = o_beg / nbk, kl1 = (o_beg + nb - 1) / nbk;
   const int nquad_k = (nbk + 3) / 4;
   const int nquad = (kl1 - kl0 + 1) * nquad_k;
   dim3 grid(nquad, s.nitems);
-  k_uvpsi<R><<<grid, 32 * UM_SPLIT, 0, s.launch_stream()>>>((const C2<R>*)in, ld_in, o_beg, nb, nbk, kl0, nquad_k,
-                                                             s.zproj64, s.Nlma, s.Nps, idx, s.atom_off, s.items,
-                                                             s.lma_list, s.iuV_d, s.Hxyz, scale_iuv ? 1 : 0, s.U);
+  k_uvpsi<R, SPLIT><<<grid, 32 * SPLIT, 0, s.launch_stream()>>>((const C2<R>*)in, ld_in, o_beg, nb, nbk, kl0, nquad_k,
+                                                                 s.zproj64, s.Nlma, s.Nps, idx, s.atom_off, s.items,
+                                                                 s.lma_list, s.iuV_d, s.Hxyz, scale_iuv ? 1 : 0, s.U);
   return cudaGetLastError();
+}
+
+template <typename R>
+static cudaError_t launch_uvpsi_t(const System& s, const void* in, int ld_in, const int* idx, int o_beg, int nb,
+                                  int nbk, bool scale_iuv) {
+  switch (s.um_split) {
+    case 1: return launch_uvpsi_split<R, 1>(s, in, ld_in, idx, o_beg, nb, nbk, scale_iuv);
+    case 2: return launch_uvpsi_split<R, 2>(s, in, ld_in, idx, o_beg, nb, nbk, scale_iuv);
+    case 8: return launch_uvpsi_split<R, 8>(s, in, ld_in, idx, o_beg, nb, nbk, scale_iuv);
+    default: return launch_uvpsi_split<R, 4>(s, in, ld_in, idx, o_beg, nb, nbk, scale_iuv);
+  }
 }
 
 cudaError_t launch_uvpsi(const System& s, const void* in, int o_beg, int nb, int nbk, bool scale_iuv, int prec) {

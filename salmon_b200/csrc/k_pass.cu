@@ -419,8 +419,14 @@ static cudaError_t launch_pass_t(const System& s, const PassIO& io, int o_beg, i
                                       s.maxpts, io.W != nullptr, s.NLx);
   auto kern = k_hpsi_pass<R, RZ, MODE>;
   if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // set outside stream capture (prepare_pass sets it before a capture)
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(s.stream, &cs);
     if (e != cudaSuccess) return e;
+    if (cs == cudaStreamCaptureStatusNone) {
+      e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+    }
   }
   dim3 grid(nb, (s.NLx + a.SX - 1) / a.SX);
   kern<<<grid, block, smem, s.launch_stream()>>>(a);
@@ -444,6 +450,24 @@ cudaError_t launch_hpsi_pass(const System& s, int mode, const PassIO& io, int o_
                : launch_pass_rz<float, 1>(s, mode, io, o_beg, nb, nbk);
   return rz2 ? launch_pass_rz<double, 2>(s, mode, io, o_beg, nb, nbk)
              : launch_pass_rz<double, 1>(s, mode, io, o_beg, nb, nbk);
+}
+
+template <typename R, int RZ>
+static cudaError_t prepare_pass_rz(const System& s) {
+  const size_t smem =
+      pass_smem_bytes(std::is_same<R, float>::value ? SGPU_PREC_C64 : SGPU_PREC_C128, s.NLy, s.NLz, s.maxpts, true, s.NLx);
+  if (smem <= 48 * 1024) return cudaSuccess;
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(k_hpsi_pass<R, RZ, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
+  if ((e = cudaFuncSetAttribute(k_hpsi_pass<R, RZ, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
+  return cudaFuncSetAttribute(k_hpsi_pass<R, RZ, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+cudaError_t prepare_pass(const System& s) {
+  const bool rz2 = (s.NLz % 2) == 0;
+  cudaError_t e = rz2 ? prepare_pass_rz<float, 2>(s) : prepare_pass_rz<float, 1>(s);
+  if (e != cudaSuccess) return e;
+  return rz2 ? prepare_pass_rz<double, 2>(s) : prepare_pass_rz<double, 1>(s);
 }
 
 int pass_block_threads(int NLy, int NLz) {

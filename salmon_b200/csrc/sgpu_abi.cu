@@ -53,6 +53,7 @@ void free_state_buffers(System* s) {
 }
 
 int alloc_state_buffers(System* s) {
+  ++s->gen;
   const size_t n = (size_t)s->norb * s->NL;
   s->elem = s->prec == SGPU_PREC_C64 ? sizeof(float2) : sizeof(double2);
   CK(cudaMalloc(&s->zu, n * s->elem));
@@ -95,10 +96,45 @@ cudaError_t apply_h(System* s, int mode, sgpu::PassIO io, int o_beg, int nb, int
 
 }  // namespace
 
-struct sgpu_system : public System {};
-
 // Entry points defined in other files report through the same message slot.
 void sgpu::set_last_error(const std::string& msg) { g_err = msg; }
+
+// One Taylor step of every resident orbital, enqueued on the handle's stream
+// (kernel launches only, so it can be captured into a CUDA graph).
+cudaError_t sgpu::enqueue_taylor_step(System& sys, double dt, bool gather_first) {
+  System* s = &sys;
+  // zfac(n) = (-i dt)^n / n!   (RT/hamiltonian.f90:46-49)
+  sgpu::PassIO io;
+  io.zfac[0][0] = 0.0;
+  io.zfac[0][1] = -dt;
+  for (int i = 2; i <= 4; ++i) {
+    const double pr = io.zfac[i - 2][0], pi = io.zfac[i - 2][1];
+    io.zfac[i - 1][0] = (pr * 0.0 - pi * (-dt)) / i;
+    io.zfac[i - 1][1] = (pr * (-dt) + pi * 0.0) / i;
+  }
+  // Each pass exports its output at the sphere points (S); the next pass's
+  // projections read S instead of gathering from the full orbitals.
+  const void* ins[4] = {s->zu, s->tw[0], s->tw[1], s->tw[2]};
+  cudaError_t e;
+  for (int n = 0; n < 4; ++n) {
+    io.in = ins[n];
+    io.S = s->nsp > 0 ? s->Sbuf : nullptr;
+    const bool from_S = s->nsp > 0 && (n > 0 || !gather_first);
+    if (n < 3) {
+      io.out = s->tw[n];
+      e = apply_h(s, 0, io, 0, s->norb, s->NBocc, -1, from_S);
+    } else {
+      io.out = nullptr;
+      io.t1 = s->tw[0];
+      io.t2 = s->tw[1];
+      io.zu = s->zu;
+      e = apply_h(s, 2, io, 0, s->norb, s->NBocc, -1, from_S);
+    }
+    if (e != cudaSuccess) return e;
+  }
+  s->S_valid = s->nsp > 0;
+  return cudaSuccess;
+}
 
 extern "C" {
 
@@ -445,34 +481,7 @@ int sgpu_hamiltonian(sgpu_handle h, double dt, int flag_current) {
   System* s = h;
   if (!s->have_state || !s->have_vloc || !s->have_proj)
     return fail(SGPU_ERR_STATE, "sgpu_hamiltonian: state, Vloc and projectors must be set first");
-  // zfac(n) = (-i dt)^n / n!   (RT/hamiltonian.f90:46-49)
-  double zr = 0.0, zi = -dt;
-  sgpu::PassIO io;
-  io.zfac[0][0] = zr; io.zfac[0][1] = zi;
-  for (int i = 2; i <= 4; ++i) {
-    const double pr = io.zfac[i - 2][0], pi = io.zfac[i - 2][1];
-    io.zfac[i - 1][0] = (pr * 0.0 - pi * (-dt)) / i;
-    io.zfac[i - 1][1] = (pr * (-dt) + pi * 0.0) / i;
-  }
-  // Each pass exports its output at the sphere points (S); the next pass's
-  // projections read S instead of gathering from the full orbitals.
-  const void* ins[4] = {s->zu, s->tw[0], s->tw[1], s->tw[2]};
-  for (int n = 0; n < 4; ++n) {
-    io.in = ins[n];
-    io.S = s->nsp > 0 ? s->Sbuf : nullptr;
-    const bool from_S = s->nsp > 0 && (n > 0 || s->S_valid);
-    if (n < 3) {
-      io.out = s->tw[n];
-      CK(apply_h(s, 0, io, 0, s->norb, s->NBocc, -1, from_S));
-    } else {
-      io.out = nullptr;
-      io.t1 = s->tw[0];
-      io.t2 = s->tw[1];
-      io.zu = s->zu;
-      CK(apply_h(s, 2, io, 0, s->norb, s->NBocc, -1, from_S));
-    }
-  }
-  s->S_valid = s->nsp > 0;
+  CK(sgpu::enqueue_taylor_step(*s, dt, !s->S_valid));
   return 0;
 }
 
@@ -792,6 +801,11 @@ extern "C" int sgpu_set_param(sgpu_handle h, int param, int value) {
       if (value < 1 || value > s->NLx) return fail(SGPU_ERR_ARG, "sgpu_set_param: nslab must be in 1..NLx");
       s->nslab = value;
       return 0;
+    case SGPU_PARAM_UVPSI_SPLIT:
+      if (value != 1 && value != 2 && value != 4 && value != 8)
+        return fail(SGPU_ERR_ARG, "sgpu_set_param: uvpsi split must be 1, 2, 4 or 8");
+      s->um_split = value;
+      return 0;
     case SGPU_PARAM_LAUNCHES:
       if (value != 0) return fail(SGPU_ERR_ARG, "sgpu_set_param: the launch counter can only be reset to 0");
       s->launches = 0;
@@ -806,6 +820,59 @@ extern "C" int sgpu_get_param(sgpu_handle h, int param, int* value) {
   switch (param) {
     case SGPU_PARAM_NSLAB: *value = h->nslab; return 0;
     case SGPU_PARAM_LAUNCHES: *value = (int)(h->launches & 0x7fffffffULL); return 0;
+    case SGPU_PARAM_UVPSI_SPLIT: *value = h->um_split; return 0;
     default: return fail(SGPU_ERR_ARG, "sgpu_get_param: unknown parameter");
   }
+}
+
+extern "C" int sgpu_autotune(sgpu_handle h, int reps, int* nslab, int* split, double* ms) {
+  if (!valid(h) || reps < 1) return fail(SGPU_ERR_ARG, "sgpu_autotune: bad argument");
+  System* s = h;
+  if (!s->have_state || !s->have_vloc || !s->have_proj)
+    return fail(SGPU_ERR_STATE, "sgpu_autotune: state, Vloc and projectors must be set first");
+  // one H application as in passes 2-3 of a Taylor step: projections from S,
+  // KB field, stencil pass with export; zu -> workspace 0 (zu is not modified)
+  sgpu::PassIO io;
+  io.in = s->zu;
+  io.out = s->tw[0];
+  io.S = s->nsp > 0 ? s->Sbuf : nullptr;
+  const bool from_S = s->nsp > 0;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const int old_slab = s->nslab, old_split = s->um_split;
+  double best = 1e300;
+  int bs = old_slab, bk = old_split;
+  cudaError_t err = cudaSuccess;
+  for (int ns : {1, 2, 4}) {
+    if (ns > 1 && s->NLx / ns < 8) continue;
+    for (int sp : {1, 2, 4, 8}) {
+      s->nslab = ns;
+      s->um_split = sp;
+      err = apply_h(s, 0, io, 0, s->norb, s->NBocc, -1, from_S);  // warm-up
+      if (err == cudaSuccess) err = cudaEventRecord(e0, s->stream);
+      for (int r = 0; r < reps && err == cudaSuccess; ++r) err = apply_h(s, 0, io, 0, s->norb, s->NBocc, -1, from_S);
+      if (err == cudaSuccess) err = cudaEventRecord(e1, s->stream);
+      if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+      float t = 0;
+      if (err == cudaSuccess) err = cudaEventElapsedTime(&t, e0, e1);
+      if (err != cudaSuccess) break;
+      if (t / reps < best) { best = t / reps; bs = ns; bk = sp; }
+    }
+    if (err != cudaSuccess) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  s->S_valid = false;  // the timed applications overwrote S
+  if (err != cudaSuccess) {
+    s->nslab = old_slab;
+    s->um_split = old_split;
+    return cuda_fail(err, "sgpu_autotune");
+  }
+  s->nslab = bs;
+  s->um_split = bk;
+  if (nslab) *nslab = bs;
+  if (split) *split = bk;
+  if (ms) *ms = best;
+  return 0;
 }

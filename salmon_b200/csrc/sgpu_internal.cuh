@@ -68,6 +68,9 @@ struct System {
   cudaStream_t stream = nullptr;
   // Kernels launched on `stream` so far (read through SGPU_PARAM_LAUNCHES).
   mutable unsigned long long launches = 0;
+  // Incremented whenever the orbital / workspace buffers are reallocated
+  // (a captured graph of the handle is then stale).
+  unsigned long long gen = 0;
   // The stream for one kernel launch; counts the launch.
   cudaStream_t launch_stream() const {
     ++launches;
@@ -161,6 +164,7 @@ struct System {
 
   // tuning
   int nslab = 1;                   // x-slabs per orbital in the stencil pass
+  int um_split = 4;                // warps splitting the points of one projection tile (1, 2, 4, 8)
 };
 
 // ------------------------------------------------------------ kernel API --
@@ -195,6 +199,9 @@ struct PassIO {
 // prec = -1 uses the handle's precision; SGPU_PREC_C128 forces FP64 (ground state).
 cudaError_t launch_hpsi_pass(const System& s, int mode, const PassIO& io, int o_beg, int nb, int nbk, int prec = -1);
 // threads per CTA of the pass kernel for an NLy x NLz plane
+// Sets the shared-memory attribute of every stencil-pass kernel the handle can
+// launch (needed before capturing its launches into a graph).
+cudaError_t prepare_pass(const System& s);
 int pass_block_threads(int NLy, int NLz);
 
 // zproj(j,ilma,k) = conj(exp(i kAc.r)) uV(j,ilma)  for the local k-points.
@@ -230,4 +237,12 @@ cudaError_t launch_rotate(const System& s, const double2* in, const double2* Z, 
 // Sets the message that sgpu_last_error returns (defined with the C ABI).
 void set_last_error(const std::string& msg);
 
+// One Taylor step of every resident orbital on the handle's stream (kernel
+// launches only).  gather_first: the first projections gather from the
+// orbitals instead of reading the sphere values S of the previous step.
+cudaError_t enqueue_taylor_step(System& s, double dt, bool gather_first);
+
 }  // namespace sgpu
+
+// The C ABI's opaque handle is the System itself.
+struct sgpu_system : public sgpu::System {};

@@ -130,6 +130,13 @@ class GpuSystem:
         call("sgpu_get_param", self._h, _lib.PARAMS[name], C.byref(v))
         return v.value
 
+    def autotune(self, reps: int = 5):
+        """Times every launch shape the library knows on the resident orbitals and
+        keeps the fastest; returns (nslab, uvpsi_split, ms per H application)."""
+        ns, sp, ms = C.c_int(), C.c_int(), C.c_double()
+        call("sgpu_autotune", self._h, int(reps), C.byref(ns), C.byref(sp), C.byref(ms))
+        return ns.value, sp.value, ms.value
+
     def time_kernel(self, kernel: str, reps: int = 10) -> float:
         """Mean device milliseconds per launch of one library kernel (CUDA events on the library stream)."""
         ms = C.c_double()
@@ -191,4 +198,34 @@ class GpuSystem:
         return ek.value, en.value
 
 
-__all__ = ["GpuSystem", "SalmonGPUError", "PRECISIONS"]
+class GpuBatch:
+    """Several GpuSystem handles advanced together, one CUDA-graph replay per call
+    of ``step`` (sgpu_batch_*)."""
+
+    def __init__(self, systems):
+        self.systems = list(systems)
+        arr = (C.c_void_p * len(self.systems))(*[g.handle for g in self.systems])
+        self._b = C.c_void_p()
+        call("sgpu_batch_create", arr, len(self.systems), C.byref(self._b))
+
+    def step(self, dts, nsteps: int = 1):
+        d = np.ascontiguousarray(np.broadcast_to(np.asarray(dts, dtype=np.float64), (len(self.systems),)))
+        call("sgpu_batch_step", self._b, _vp(d), int(nsteps))
+
+    @property
+    def stream(self) -> int:
+        return _lib.lib().sgpu_batch_stream(self._b) or 0
+
+    def close(self):
+        if self._b:
+            call("sgpu_batch_destroy", self._b)
+            self._b = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+__all__ = ["GpuSystem", "GpuBatch", "SalmonGPUError", "PRECISIONS"]

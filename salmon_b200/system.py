@@ -372,6 +372,49 @@ def microbench_system(N: int, nkgrid=(4, 4, 4), Nb: int = 32, A=(1e-2, 0.0, 0.0)
     return sysm, kAc, vloc, zu
 
 
+def si_supercell_system(ncell=(1, 1, 1), grid=(16, 16, 16), nkgrid=(4, 4, 4), Nb: int = 16, A=(0.0, 0.0, 0.0),
+                        a: float = 10.26, seed: int = SEED, with_orbitals: bool = True):
+    """Diamond-Si supercell of ncell cubic 8-atom cells (a = 10.26 bohr) on the
+    given grid: 8*prod(ncell) atoms x {s,px,py,pz} Gaussian projectors (r_c =
+    R_ps = 2 bohr), V_loc = seeded periodic Gaussians on the atoms, uniform
+    nkgrid k-points, Nb bands.  The shapes of the Si8 / Si16 / Si64 systems:
+    ncell (1,1,1) 16^3, (1,1,2) 16x16x32, (2,2,2) 32^3.
+    Returns (system, kAc (3,NK), Vloc (NL,), zu (nk,Nb,NL) complex128 or None)."""
+    rng = np.random.default_rng(seed)
+    nc = np.asarray(ncell)
+    aL = a * nc.astype(np.float64)
+    NLx, NLy, NLz = grid
+    bl = 2 * np.pi / aL
+    kAc0 = uniform_k_grid(*nkgrid, bl)
+    NK = kAc0.shape[1]
+    occ = np.full((NK, Nb), 2.0 / NK)
+    cells = np.array([[i, j, k] for i in range(nc[0]) for j in range(nc[1]) for k in range(nc[2])])
+    Rion = np.concatenate([(DIAMOND_RED + c) * a for c in cells])
+    Mps, Jxyz, Jxx, Jyy, Jzz, dist = calc_jxyz(NLx, NLy, NLz, aL, Rion, 2.0)
+    Hxyz = float(np.prod(aL / np.array(grid)))
+    uV, iuV, a_tbl = gaussian_projectors(Mps, dist, Hxyz)
+    depth = rng.uniform(0.5, 2.0, Rion.shape[0])
+    width = rng.uniform(1.0, 2.0, Rion.shape[0])
+    vloc = periodic_gaussian_vloc(NLx, NLy, NLz, aL, Rion, depth, width)
+    sysm = System(NLx=NLx, NLy=NLy, NLz=NLz, aL=aL, kAc0=kAc0, NB=Nb, NBoccmax=Nb, occ=occ, Rion=Rion, Rps=2.0,
+                  Mps=Mps, Jxyz=Jxyz, Jxx=Jxx, Jyy=Jyy, Jzz=Jzz, uV=uV, iuV=iuV, a_tbl=a_tbl)
+    sysm.extra.update(seed=seed, depth=depth, width=width)
+    kAc = np.ascontiguousarray(kAc0 + np.asarray(A, dtype=np.float64)[:, None])
+    zu = None
+    if with_orbitals:
+        NL = NLx * NLy * NLz
+        zu = rng.standard_normal((NK, Nb, NL)) + 1j * rng.standard_normal((NK, Nb, NL))
+        zu = orthonormalise(zu, Hxyz)
+    return sysm, kAc, vloc, zu
+
+
+BATCHED_SYSTEMS = {  # name: (ncell, grid, nkgrid, bands)
+    "Si8": ((1, 1, 1), (16, 16, 16), (4, 4, 4), 16),
+    "Si16": ((1, 1, 2), (16, 16, 32), (4, 4, 2), 32),
+    "Si64": ((2, 2, 2), (32, 32, 32), (2, 2, 2), 128),
+}
+
+
 def small_system(NLx=8, NLy=8, NLz=10, nk=3, nb=4, a=(6.0, 6.5, 7.0), nat=2, seed=7, Rps=1.6):
     """A small non-cubic system with ragged sizes for exhaustive parity tests:
     uneven grid, few k-points and bands, random atom sites, Gaussian projectors."""
