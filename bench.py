@@ -55,6 +55,8 @@ def parse():
     p.add_argument("--only", choices=["c128", "c64"], help="run one precision (profiling)")
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling)")
     p.add_argument("--no-precision", action="store_true", help="skip the FP32-vs-FP64 J(t) run")
+    p.add_argument("--no-batched", action="store_true", help="skip the batched-systems run")
+    p.add_argument("--batched-steps", type=int, default=1000)
     return p.parse_args()
 
 
@@ -192,6 +194,63 @@ def precision_check(nsteps=500):
                         "J every step (FP64 reductions)", "target": 1e-5}
 
 
+def batched_bench(nsteps=1000, per_replay=10):
+    """Si8 (16^3, 64 k x 16 b), Si16 (16x16x32, 32 k x 32 b) and Si64 (32^3, 8 k x
+    128 b) in complex(4), launch shapes autotuned per system, advanced together by
+    graph replays of `per_replay` Taylor steps; beside it the same systems stepped
+    one sgpu_hamiltonian call at a time."""
+    import torch
+    from salmon_b200 import system as S
+    from salmon_b200.rt import GpuBatch, GpuSystem
+    gs, tuned, norb = [], {}, 0
+    for name, (cells, grid, nkg, nb) in S.BATCHED_SYSTEMS.items():
+        sysm, kAc, vloc, zu = S.si_supercell_system(cells, grid, nkg, nb, A=(1e-2, 0.0, 0.0))
+        g = GpuSystem(sysm, "c64")
+        g.set_state(zu)
+        g.set_vloc(vloc)
+        g.update_projector(kAc)
+        ns, sp, ms = g.autotune(reps=3)
+        tuned[name] = {"nslab": ns, "uvpsi_split": sp, "ms_per_h_apply": ms, "norb": sysm.nk_local * nb,
+                       "grid": list(grid)}
+        norb += sysm.nk_local * nb
+        gs.append(g)
+    dts = [DT] * len(gs)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with GpuBatch(gs) as b:
+        st = torch.cuda.ExternalStream(b.stream)
+        for _ in range(3):
+            b.step(dts, per_replay)
+        for g in gs:
+            g.synchronize()
+        torch.cuda.synchronize()
+        reps = max(1, nsteps // per_replay)
+        e0.record(st)
+        for _ in range(reps):
+            b.step(dts, per_replay)
+        e1.record(st)
+        e1.synchronize()
+        ms_graph = e0.elapsed_time(e1) / (reps * per_replay)
+    # one call at a time, same systems and shapes (host wall clock after a sync)
+    nseq = max(10, nsteps // 10)
+    for g in gs:
+        g.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(nseq):
+        for g in gs:
+            g.hamiltonian(DT)
+    for g in gs:
+        g.synchronize()
+    ms_seq = (time.perf_counter() - t0) * 1e3 / nseq
+    for g in gs:
+        g.close()
+    return {"value": norb / (ms_graph * 1e-3), "unit": "orbital-updates/s", "ms_per_step": ms_graph,
+            "steps": reps * per_replay, "steps_per_graph_replay": per_replay,
+            "sequential_ms_per_step": ms_seq, "graph_speedup": ms_seq / ms_graph, "systems": tuned,
+            "workload": "Si8 16^3 64k x16b + Si16 16x16x32 32k x32b + Si64 32^3 8k x128b, complex(4), "
+                        "synthetic Gaussian projectors / V_loc"}
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -325,6 +384,9 @@ def main():
     prec_check = None
     if rank == 0 and not (args.only or args.no_e2e or args.no_precision):
         prec_check = precision_check()
+    batched = None
+    if rank == 0 and not (args.only or args.no_e2e or args.no_batched):
+        batched = batched_bench(args.batched_steps)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -359,6 +421,7 @@ def main():
             "e2e": h["e2e"],
             "gpu_launches": h["launches"],
             "precision": prec_check,
+            "batched": batched,
             "clocks": clocks,
         }
         print(json.dumps(out))
