@@ -226,6 +226,17 @@ int sgpu_gram_schmidt(sgpu_handle h);
  * band (may be NULL).  Replaces CG_ompk (GS/CG.f90:34-139). */
 int sgpu_cg(sgpu_handle h, int ncg, double* esp_var, int* iters);
 
+/* CG stops iterating a band once its Rayleigh quotient changes by less than
+ * delta_cg between iterations; the reference fixes delta_cg = 1e-15
+ * (GS/CG.f90:42, :114), which is also the default here.  A smaller value lets
+ * CG drive residual norms below ~1e-7. */
+int sgpu_set_cg_delta(sgpu_handle h, double delta_cg);
+
+/* Residual norms sqrt(||H u - <u|H|u> u||^2 Hxyz) of every band after the last
+ * sgpu_cg, HOST (NB,NK_s:NK_e), without the occupation factor of esp_var (so
+ * empty bands are reported too).  No reference counterpart. */
+int sgpu_cg_residuals(sgpu_handle h, double* res);
+
 /* Subspace diagonalisation: H_sub(NB,NB) per k-point, its Hermitian
  * eigen-decomposition (ascending eigenvalues) and the rotation of the bands.
  * esp (NB,NK_s:NK_e) HOST receives the eigenvalues (may be NULL).  Replaces
@@ -241,8 +252,17 @@ int sgpu_gs_to_rt(sgpu_handle h);
 enum {
   SGPU_PARAM_NSLAB = 0,       /* CTAs per orbital along x in the stencil pass (1..NLx)              */
   SGPU_PARAM_LAUNCHES = 1,    /* kernels the handle has launched, modulo 2^31 (read; set 0 to reset) */
-  SGPU_PARAM_UVPSI_SPLIT = 2  /* warps splitting the points of one projection tile: 1, 2, 4 or 8     */
+  SGPU_PARAM_UVPSI_SPLIT = 2, /* warps splitting the points of one projection tile: 1, 2, 4 or 8     */
+  SGPU_PARAM_CG_PRECOND = 3   /* sgpu_cg direction: SGPU_CG_PLAIN, SGPU_CG_TPA or SGPU_CG_LEARNED     */
 };
+
+/* CG preconditioners.  PLAIN is the reference's CG_ompk.  TPA multiplies the
+ * gradient in reciprocal space by the Teter-Payne-Allan kinetic-energy factor
+ * (Phys. Rev. B 40, 12255 (1989)); LEARNED applies the loaded 3D-convolution
+ * network (sgpu_net_*) to the TPA-preconditioned gradient, as a learned
+ * refinement of it (so TPA is what remains without a network).  Neither has a
+ * reference counterpart. */
+enum { SGPU_CG_PLAIN = 0, SGPU_CG_TPA = 1, SGPU_CG_LEARNED = 2 };
 
 /* Sets / reads a launch parameter of the handle (the autotuner's knobs).  No
  * reference counterpart; the nearest is auto_blocking
@@ -257,6 +277,33 @@ int sgpu_get_param(sgpu_handle h, int param, int* value);
  * modified.  No reference counterpart; the nearest is auto_blocking
  * (modules/opt_variables.f90:340-353). */
 int sgpu_autotune(sgpu_handle h, int reps, int* nslab, int* split, double* ms_per_apply);
+
+/* ---- CG preconditioners (ground state) ------------------------------------ */
+/* The TPA preconditioner applied to nvec DEV complex(8) vectors (layout
+ * [nvec][NL]); vector v is taken at local k-point kidx[v] (HOST, 0-based; NULL
+ * means v) with band kinetic energy tband[v] (HOST).  Test and training hook;
+ * sgpu_cg applies the same kernels internally. */
+int sgpu_tpa_apply(sgpu_handle h, const void* in_dev, void* out_dev, int nvec, const int* kidx, const double* tband);
+
+/* The learned preconditioner: a 3D convolution network on the periodic grid
+ * (conv 1->8, 8->8, 8->1 channels; 3x3x3 kernels with circular padding; no bias
+ * or activation), BF16 weights and activations with FP32 accumulation.  It is
+ * applied to the real and the imaginary part of a complex vector separately
+ * (each scaled by the vector's 1/rms), so K(c g) = c K(g) for complex c.
+ * Weights: sgpu_net_weight_count() floats, layer by layer, each [co][ci][tap],
+ * tap = (dx+1)*9 + (dy+1)*3 + (dz+1).  No reference counterpart. */
+int sgpu_net_weight_count(void);
+int sgpu_net_set_weights(sgpu_handle h, const float* w);   /* HOST; resets the optimiser */
+int sgpu_net_get_weights(sgpu_handle h, float* w);         /* HOST */
+/* out = K(in) for nvec DEV complex(8) vectors [nvec][NL] */
+int sgpu_net_apply(sgpu_handle h, const void* in_dev, void* out_dev, int nvec);
+/* Mean squared error of K(g) against targets t (both DEV complex(8)
+ * [nvec][NL], t scaled like g) and its gradient with respect to the weights
+ * (grad HOST, may be NULL; loss HOST, may be NULL). */
+int sgpu_net_grad(sgpu_handle h, const void* g_dev, const void* t_dev, int nvec, float* grad, double* loss);
+/* One Adam step (learning rate lr) on that loss; loss HOST (may be NULL) is the
+ * loss before the step. */
+int sgpu_net_train_step(sgpu_handle h, const void* g_dev, const void* t_dev, int nvec, float lr, double* loss);
 
 /* ---- batched systems ------------------------------------------------------ */
 /* Several systems (handles on the current device) advanced together.  No

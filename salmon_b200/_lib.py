@@ -44,6 +44,15 @@ ABI = {
     "sgpu_gs_to_rt": (C.c_int, [_vp]),
     "sgpu_set_param": (C.c_int, [_vp, _ip, _ip]),
     "sgpu_get_param": (C.c_int, [_vp, _ip, C.POINTER(C.c_int)]),
+    "sgpu_cg_residuals": (C.c_int, [_vp, _vp]),
+    "sgpu_set_cg_delta": (C.c_int, [_vp, C.c_double]),
+    "sgpu_tpa_apply": (C.c_int, [_vp, _vp, _vp, _ip, _vp, _vp]),
+    "sgpu_net_weight_count": (C.c_int, []),
+    "sgpu_net_set_weights": (C.c_int, [_vp, _vp]),
+    "sgpu_net_get_weights": (C.c_int, [_vp, _vp]),
+    "sgpu_net_apply": (C.c_int, [_vp, _vp, _vp, _ip]),
+    "sgpu_net_grad": (C.c_int, [_vp, _vp, _vp, _ip, _vp, _dp]),
+    "sgpu_net_train_step": (C.c_int, [_vp, _vp, _vp, _ip, C.c_float, _dp]),
     "sgpu_autotune": (C.c_int, [_vp, _ip, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]),
     "sgpu_batch_create": (C.c_int, [C.POINTER(C.c_void_p), _ip, C.POINTER(C.c_void_p)]),
     "sgpu_batch_step": (C.c_int, [_vp, _vp, _ip]),
@@ -51,7 +60,7 @@ ABI = {
     "sgpu_batch_destroy": (C.c_int, [_vp]),
 }
 
-PARAMS = {"nslab": 0, "launches": 1, "uvpsi_split": 2}
+PARAMS = {"nslab": 0, "launches": 1, "uvpsi_split": 2, "cg_precond": 3}
 
 KERNELS = {"stencil_pass": 0, "taylor_last": 1, "uvpsi": 2, "psi_rho": 3, "kb_field": 4}
 

@@ -66,7 +66,7 @@ cudaError_t launch_gram_schmidt(const System& s, double2* zu) {
 // the H applications; one CTA per k-point works on band ib of its k-point.
 // Work vectors W[which][k][NL] (which = xk, hxk, txk, gk, pk, pko, htpsi, ttpsi):
 // each kind is a contiguous batch of one vector per k-point for the H pass.
-enum { CG_XK = 0, CG_HXK, CG_TXK, CG_GK, CG_PK, CG_PKO, CG_HT, CG_TT, CG_NW };
+enum { CG_XK = 0, CG_HXK, CG_TXK, CG_GK, CG_PK, CG_PKO, CG_HT, CG_TT, CG_HK, CG_NW };
 
 struct CGState {
   double xkHxk, gkgk;
@@ -142,9 +142,75 @@ __global__ void __launch_bounds__(GS_THREADS) k_cg_pre(const double2* __restrict
   for (int i = threadIdx.x; i < NL; i += blockDim.x) pko[i] = make_double2(pko[i].x * inv, pko[i].y * inv);
 }
 
+// Preconditioned variant (no reference counterpart; Payne et al., Rev. Mod.
+// Phys. 64, 1045 (1992), section V.B): the gradient gk (as above, orthogonal
+// to the lower bands) is preconditioned into hk = K gk by a separate kernel
+// chain; k_cg_dir orthogonalises hk against the lower bands and xk, and builds
+// the conjugate direction with beta = <gk|hk> / <gk|hk>_previous.
+// k_cg_grad also records the kinetic energy of xk (T_band, for the TPA form).
+__global__ void __launch_bounds__(GS_THREADS) k_cg_grad(const double2* __restrict__ zu, double2* __restrict__ W,
+                                                        CGState* __restrict__ st, double* __restrict__ tband, int ib,
+                                                        int NB, int NL, double Hxyz) {
+  __shared__ double sh[64];
+  const int k = blockIdx.x;
+  if (st[k].done) return;
+  const double2* base = zu + (size_t)k * NB * NL;
+  double2 *xk = wv(W, k, CG_XK, NL), *hxk = wv(W, k, CG_HXK, NL), *gk = wv(W, k, CG_GK, NL);
+  double2* hk = wv(W, k, CG_HK, NL);
+  const double xkHxk = st[k].xkHxk;
+  for (int i = threadIdx.x; i < NL; i += blockDim.x)
+    gk[i] = make_double2(hxk[i].x - xkHxk * xk[i].x, hxk[i].y - xkHxk * xk[i].y);
+  for (int ibt = 0; ibt < ib; ++ibt) {
+    const double2* ut = base + (size_t)ibt * NL;
+    const double2 d = blk_zdot(ut, gk, NL, sh);
+    const double2 zs = make_double2(d.x * Hxyz, d.y * Hxyz);
+    for (int i = threadIdx.x; i < NL; i += blockDim.x) gk[i] = csub(gk[i], cmul(ut[i], zs));
+  }
+  for (int i = threadIdx.x; i < NL; i += blockDim.x) hk[i] = gk[i];  // the preconditioner works in place on hk
+  const double t = blk_zdot(xk, wv(W, k, CG_TXK, NL), NL, sh).x * Hxyz;
+  if (threadIdx.x == 0) tband[k] = t;
+}
+
+__global__ void __launch_bounds__(GS_THREADS) k_cg_dir(const double2* __restrict__ zu, double2* __restrict__ W,
+                                                       CGState* __restrict__ st, int ib, int iter, int NB, int NL,
+                                                       double Hxyz) {
+  __shared__ double sh[64];
+  const int k = blockIdx.x;
+  if (st[k].done) return;
+  const double2* base = zu + (size_t)k * NB * NL;
+  double2 *xk = wv(W, k, CG_XK, NL), *gk = wv(W, k, CG_GK, NL), *hk = wv(W, k, CG_HK, NL);
+  double2 *pk = wv(W, k, CG_PK, NL), *pko = wv(W, k, CG_PKO, NL);
+  for (int ibt = 0; ibt < ib; ++ibt) {
+    const double2* ut = base + (size_t)ibt * NL;
+    const double2 d = blk_zdot(ut, hk, NL, sh);
+    const double2 zs = make_double2(d.x * Hxyz, d.y * Hxyz);
+    for (int i = threadIdx.x; i < NL; i += blockDim.x) hk[i] = csub(hk[i], cmul(ut[i], zs));
+  }
+  {
+    const double2 d = blk_zdot(xk, hk, NL, sh);
+    const double2 zs = make_double2(d.x * Hxyz, d.y * Hxyz);
+    for (int i = threadIdx.x; i < NL; i += blockDim.x) hk[i] = csub(hk[i], cmul(xk[i], zs));
+  }
+  const double s = blk_zdot(gk, hk, NL, sh).x * Hxyz;
+  if (iter == 1) {
+    for (int i = threadIdx.x; i < NL; i += blockDim.x) pk[i] = hk[i];
+  } else {
+    const double uk = s / st[k].gkgk;
+    for (int i = threadIdx.x; i < NL; i += blockDim.x)
+      pk[i] = make_double2(hk[i].x + uk * pk[i].x, hk[i].y + uk * pk[i].y);
+  }
+  __syncthreads();  // every thread has read gkgk
+  if (threadIdx.x == 0) st[k].gkgk = s;
+  const double2 d = blk_zdot(xk, pk, NL, sh);
+  const double2 zs = make_double2(d.x * Hxyz, d.y * Hxyz);
+  for (int i = threadIdx.x; i < NL; i += blockDim.x) pko[i] = csub(pk[i], cmul(xk[i], zs));
+  const double inv = 1.0 / sqrt(blk_nrm2(pko, NL, sh) * Hxyz);
+  for (int i = threadIdx.x; i < NL; i += blockDim.x) pko[i] = make_double2(pko[i].x * inv, pko[i].y * inv);
+}
+
 // 2x2 Rayleigh-Ritz in span{xk, pko} and the update (CG.f90:108-119)
 __global__ void __launch_bounds__(GS_THREADS) k_cg_post(double2* __restrict__ W, CGState* __restrict__ st, int iter,
-                                                        int NL, double Hxyz) {
+                                                        int NL, double Hxyz, double delta_cg) {
   __shared__ double sh[64];
   const int k = blockIdx.x;
   if (st[k].done) return;
@@ -161,7 +227,7 @@ __global__ void __launch_bounds__(GS_THREADS) k_cg_post(double2* __restrict__ W,
   cx = make_double2(cx.x * cp, cx.y * cp);
   __syncthreads();
   if (threadIdx.x == 0) st[k].iters = iter;
-  if (fabs(ev - xkHxk) < 1.e-15) {  // delta_cg (CG.f90:42,114)
+  if (fabs(ev - xkHxk) < delta_cg) {  // delta_cg = 1e-15 in the reference (CG.f90:42,114)
     if (threadIdx.x == 0) st[k].done = 1;
     return;
   }
@@ -191,8 +257,8 @@ __global__ void __launch_bounds__(GS_THREADS) k_cg_end(double2* __restrict__ zu,
 
 // esp_var(ib,k) = sqrt(||H u - <u|H u> u||^2 Hxyz) occ(ib,k)  (CG.f90:124-126)
 __global__ void __launch_bounds__(GS_THREADS) k_cg_resid(double2* __restrict__ W, const double* __restrict__ occ_gs,
-                                                         double* __restrict__ esp_var, int ib, int NB, int NL,
-                                                         double Hxyz) {
+                                                         double* __restrict__ esp_var, double* __restrict__ res,
+                                                         int ib, int NB, int NL, double Hxyz) {
   __shared__ double sh[64];
   const int k = blockIdx.x;
   const double2 *u = wv(W, k, CG_XK, NL), *ht = wv(W, k, CG_HT, NL);
@@ -203,7 +269,10 @@ __global__ void __launch_bounds__(GS_THREADS) k_cg_resid(double2* __restrict__ W
     v[0] = fma(r.x, r.x, fma(r.y, r.y, v[0]));
   }
   block_allsum<1>(v, sh);
-  if (threadIdx.x == 0) esp_var[(size_t)k * NB + ib] = sqrt(v[0] * Hxyz) * occ_gs[(size_t)k * NB + ib];
+  if (threadIdx.x == 0) {
+    esp_var[(size_t)k * NB + ib] = sqrt(v[0] * Hxyz) * occ_gs[(size_t)k * NB + ib];
+    res[(size_t)k * NB + ib] = sqrt(v[0] * Hxyz);  // the residual norm itself, for convergence tests
+  }
 }
 
 cudaError_t launch_cg_begin(const System& s, double2* zu, double2* W, void* st, int ib) {
@@ -219,15 +288,23 @@ cudaError_t launch_cg_pre(const System& s, const double2* zu, double2* W, void* 
   return cudaGetLastError();
 }
 cudaError_t launch_cg_post(const System& s, double2* W, void* st, int iter) {
-  k_cg_post<<<s.nkl, GS_THREADS, 0, s.launch_stream()>>>(W, (CGState*)st, iter, s.NL, s.Hxyz);
+  k_cg_post<<<s.nkl, GS_THREADS, 0, s.launch_stream()>>>(W, (CGState*)st, iter, s.NL, s.Hxyz, s.cg_delta);
   return cudaGetLastError();
 }
 cudaError_t launch_cg_end(const System& s, double2* zu, double2* W, int ib) {
   k_cg_end<<<s.nkl, GS_THREADS, 0, s.launch_stream()>>>(zu, W, ib, s.NB, s.NL, s.Hxyz);
   return cudaGetLastError();
 }
-cudaError_t launch_cg_resid(const System& s, double2* W, const double* occ_gs, double* esp_var, int ib) {
-  k_cg_resid<<<s.nkl, GS_THREADS, 0, s.launch_stream()>>>(W, occ_gs, esp_var, ib, s.NB, s.NL, s.Hxyz);
+cudaError_t launch_cg_grad(const System& s, const double2* zu, double2* W, void* st, double* tband, int ib) {
+  k_cg_grad<<<s.nkl, GS_THREADS, 0, s.launch_stream()>>>(zu, W, (CGState*)st, tband, ib, s.NB, s.NL, s.Hxyz);
+  return cudaGetLastError();
+}
+cudaError_t launch_cg_dir(const System& s, const double2* zu, double2* W, void* st, int ib, int iter) {
+  k_cg_dir<<<s.nkl, GS_THREADS, 0, s.launch_stream()>>>(zu, W, (CGState*)st, ib, iter, s.NB, s.NL, s.Hxyz);
+  return cudaGetLastError();
+}
+cudaError_t launch_cg_resid(const System& s, double2* W, const double* occ_gs, double* esp_var, double* res, int ib) {
+  k_cg_resid<<<s.nkl, GS_THREADS, 0, s.launch_stream()>>>(W, occ_gs, esp_var, res, ib, s.NB, s.NL, s.Hxyz);
   return cudaGetLastError();
 }
 size_t cg_state_bytes() { return sizeof(CGState); }

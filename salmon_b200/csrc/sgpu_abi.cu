@@ -365,13 +365,14 @@ int sgpu_destroy(sgpu_handle h) {
   if (!h) return 0;
   System* s = h;
   if (s->stream) cudaStreamSynchronize(s->stream);
+  sgpu::net_free(*s);
   free_state_buffers(s);
   void* bufs[] = {s->vloc64, s->vloc32, s->occ_o, s->kAc_d, s->idx_proj, s->atom_off, s->rpos, s->items,
                   s->lma_list, s->iuV_d, s->lma_atom, s->uV_d, s->zproj64, s->zproj32, s->sp_off, s->rec, s->cont, s->qmap, s->kbq, s->kb_multi, s->lqi, s->Sbuf, s->Wbuf,
                   s->U, s->Uw, s->red, s->stage};
   for (void* p : bufs) cudaFree(p);
   void* gbufs[] = {s->gs_zu, s->gs_aux, s->gs_W, s->gs_st, s->gs_part, s->gs_A, s->gs_V, s->gs_w, s->gs_sweeps,
-                   s->occ_gs, s->gs_out};
+                   s->occ_gs, s->gs_out, s->gs_res, s->gs_tb};
   for (void* p : gbufs) cudaFree(p);
   if (s->gs_h) cudaFreeHost(s->gs_h);
   if (s->red_h) cudaFreeHost(s->red_h);
@@ -639,6 +640,9 @@ int gs_alloc(System* s) {
   CK(cudaMalloc(&s->gs_w, (size_t)s->nkl * s->NB * sizeof(double)));
   CK(cudaMalloc(&s->gs_sweeps, (size_t)s->nkl * sizeof(int)));
   CK(cudaMalloc(&s->gs_out, (size_t)s->nkl * s->NB * sizeof(double)));
+  CK(cudaMalloc(&s->gs_res, (size_t)s->nkl * s->NB * sizeof(double)));
+  CK(cudaMemsetAsync(s->gs_res, 0, (size_t)s->nkl * s->NB * sizeof(double), s->stream));
+  CK(cudaMalloc(&s->gs_tb, (size_t)s->nkl * sizeof(double)));
   CK(cudaMallocHost((void**)&s->gs_h, (size_t)s->nkl * s->NB * sizeof(double)));
   std::vector<double> occ((size_t)s->nkl * s->NB);
   for (int kl = 0; kl < s->nkl; ++kl)
@@ -737,13 +741,20 @@ int sgpu_cg(sgpu_handle h, int ncg, double* esp_var, int* iters) {
     if ((rc = gs_hpsi(s, vec(0), vec(1), vec(2), s->nkl, 1))) return rc;   // xk -> hxk, txk
     CK(sgpu::launch_cg_dot0(*s, W, s->gs_st));
     for (int iter = 1; iter <= ncg; ++iter) {
-      CK(sgpu::launch_cg_pre(*s, s->gs_zu, W, s->gs_st, ib, iter));
+      if (s->cg_precond == 0) {  // the reference's CG (CG.f90:85-106)
+        CK(sgpu::launch_cg_pre(*s, s->gs_zu, W, s->gs_st, ib, iter));
+      } else {                   // preconditioned direction
+        CK(sgpu::launch_cg_grad(*s, s->gs_zu, W, s->gs_st, s->gs_tb, ib));
+        CK(sgpu::launch_tpa(*s, vec(8), s->nkl, s->gs_tb, 1));                      // kinetic-energy factor
+        if (s->cg_precond == 2) CK(sgpu::launch_precond_net(*s, vec(8), s->nkl));  // learned refinement
+        CK(sgpu::launch_cg_dir(*s, s->gs_zu, W, s->gs_st, ib, iter));
+      }
       if ((rc = gs_hpsi(s, vec(5), vec(6), vec(7), s->nkl, 1))) return rc; // pko -> htpsi, ttpsi
       CK(sgpu::launch_cg_post(*s, W, s->gs_st, iter));
     }
     CK(sgpu::launch_cg_end(*s, s->gs_zu, W, ib));
     if ((rc = gs_hpsi(s, vec(0), vec(6), nullptr, s->nkl, 1))) return rc;  // H u_ib
-    CK(sgpu::launch_cg_resid(*s, W, s->occ_gs, s->gs_out, ib));
+    CK(sgpu::launch_cg_resid(*s, W, s->occ_gs, s->gs_out, s->gs_res, ib));
     if (iters) {
       CK(cudaMemcpyAsync(st_h.data(), s->gs_st, st_h.size(), cudaMemcpyDeviceToHost, s->stream));
       CK(cudaStreamSynchronize(s->stream));
@@ -758,6 +769,19 @@ int sgpu_cg(sgpu_handle h, int ncg, double* esp_var, int* iters) {
   if (iters) std::memcpy(iters, it_all.data(), it_all.size() * sizeof(int));
   CK(cudaStreamSynchronize(s->stream));
   return 0;
+}
+
+int sgpu_set_cg_delta(sgpu_handle h, double delta_cg) {
+  if (!valid(h) || !(delta_cg > 0.0)) return fail(SGPU_ERR_ARG, "sgpu_set_cg_delta: need a positive threshold");
+  h->cg_delta = delta_cg;
+  return 0;
+}
+
+int sgpu_cg_residuals(sgpu_handle h, double* res) {
+  if (!valid(h) || !res) return fail(SGPU_ERR_ARG, "sgpu_cg_residuals: null argument");
+  System* s = h;
+  if (!s->have_gs) return fail(SGPU_ERR_STATE, "sgpu_cg_residuals: no ground-state orbitals loaded");
+  return gs_copy_out(s, s->gs_res, res);
 }
 
 int sgpu_subspace_diag(sgpu_handle h, double* esp) {
@@ -801,6 +825,13 @@ extern "C" int sgpu_set_param(sgpu_handle h, int param, int value) {
       if (value < 1 || value > s->NLx) return fail(SGPU_ERR_ARG, "sgpu_set_param: nslab must be in 1..NLx");
       s->nslab = value;
       return 0;
+    case SGPU_PARAM_CG_PRECOND:
+      if (value < 0 || value > 2) return fail(SGPU_ERR_ARG, "sgpu_set_param: CG preconditioner must be 0, 1 or 2");
+      if (value >= 1 && !(sgpu::fft_size_ok(s->NLx) && sgpu::fft_size_ok(s->NLy) && sgpu::fft_size_ok(s->NLz)))
+        return fail(SGPU_ERR_UNSUPPORTED, "sgpu_set_param: the TPA preconditioner needs grid sizes 2^a 3^b <= 96");
+      if (value == 2 && !s->net_ready) return fail(SGPU_ERR_STATE, "sgpu_set_param: no preconditioner network loaded");
+      s->cg_precond = value;
+      return 0;
     case SGPU_PARAM_UVPSI_SPLIT:
       if (value != 1 && value != 2 && value != 4 && value != 8)
         return fail(SGPU_ERR_ARG, "sgpu_set_param: uvpsi split must be 1, 2, 4 or 8");
@@ -821,6 +852,7 @@ extern "C" int sgpu_get_param(sgpu_handle h, int param, int* value) {
     case SGPU_PARAM_NSLAB: *value = h->nslab; return 0;
     case SGPU_PARAM_LAUNCHES: *value = (int)(h->launches & 0x7fffffffULL); return 0;
     case SGPU_PARAM_UVPSI_SPLIT: *value = h->um_split; return 0;
+    case SGPU_PARAM_CG_PRECOND: *value = h->cg_precond; return 0;
     default: return fail(SGPU_ERR_ARG, "sgpu_get_param: unknown parameter");
   }
 }

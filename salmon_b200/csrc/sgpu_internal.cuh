@@ -165,6 +165,12 @@ struct System {
   // tuning
   int nslab = 1;                   // x-slabs per orbital in the stencil pass
   int um_split = 4;                // warps splitting the points of one projection tile (1, 2, 4, 8)
+  int cg_precond = 0;              // ground-state CG preconditioner: 0 none, 1 TPA, 2 learned
+  double cg_delta = 1e-15;         // CG stops a band when its Rayleigh quotient moves less than this
+  bool net_ready = false;          // a preconditioner network has been loaded
+  void* net = nullptr;             // its weights, optimiser state and workspace (k_net.cu)
+  double* gs_tb = nullptr;         // [nkl] kinetic energy of the band in CG (TPA)
+  double* gs_res = nullptr;        // [nkl][NB] residual norms of the last sgpu_cg
 };
 
 // ------------------------------------------------------------ kernel API --
@@ -226,7 +232,20 @@ cudaError_t launch_cg_dot0(const System& s, double2* W, void* st);
 cudaError_t launch_cg_pre(const System& s, const double2* zu, double2* W, void* st, int ib, int iter);
 cudaError_t launch_cg_post(const System& s, double2* W, void* st, int iter);
 cudaError_t launch_cg_end(const System& s, double2* zu, double2* W, int ib);
-cudaError_t launch_cg_resid(const System& s, double2* W, const double* occ_gs, double* esp_var, int ib);
+cudaError_t launch_cg_resid(const System& s, double2* W, const double* occ_gs, double* esp_var, double* res, int ib);
+cudaError_t launch_cg_grad(const System& s, const double2* zu, double2* W, void* st, double* tband, int ib);
+cudaError_t launch_cg_dir(const System& s, const double2* zu, double2* W, void* st, int ib, int iter);
+// Batched 3D FFT (sign -1 forward, +1 backward; normalise divides by NL) of
+// nvec grid functions, and the TPA preconditioner applied in place to nvec
+// vectors (vector v belongs to k-point v / vecs_per_k; tband_dev[v] its band's
+// kinetic energy).  Sizes 2^a 3^b up to 96 per axis.
+bool fft_size_ok(int n);
+// The learned preconditioner applied in place to nvec vectors (k_net.cu).
+cudaError_t launch_precond_net(const System& s, double2* data, int nvec);
+void net_free(System& s);
+cudaError_t launch_fft3d(const System& s, double2* data, int nvec, int sign, bool normalise);
+cudaError_t launch_tpa(const System& s, double2* data, int nvec, const double* tband_dev, int vecs_per_k,
+                       const int* kidx_dev = nullptr);
 size_t cg_state_bytes();
 int cg_work_vectors();
 cudaError_t launch_subspace_h(const System& s, const double2* U, const double2* HU, double2* part, int nsplit,

@@ -179,6 +179,59 @@ class GpuSystem:
     def gs_to_rt(self):
         call("sgpu_gs_to_rt", self._h)
 
+    def cg_residuals(self):
+        """Residual norms (nkl, NB) of every band after the last ``cg`` (no occupation factor)."""
+        s = self.sysm
+        r = np.empty((s.nk_local, s.NB))
+        call("sgpu_cg_residuals", self._h, _vp(r))
+        return r
+
+    def set_cg_delta(self, delta_cg: float):
+        """Per-band CG stopping threshold on the Rayleigh quotient (reference: 1e-15)."""
+        call("sgpu_set_cg_delta", self._h, C.c_double(delta_cg))
+
+    def set_cg_preconditioner(self, kind: str):
+        """'plain' (the reference's CG), 'tpa' or 'learned' (needs ``net_set_weights``)."""
+        self.set_param("cg_precond", {"plain": 0, "tpa": 1, "learned": 2}[kind])
+
+    def tpa_apply(self, in_dev: int, out_dev: int, nvec: int, tband, kidx=None):
+        """TPA on nvec device vectors; vector v at local k-point kidx[v] (default v)."""
+        tb = np.ascontiguousarray(tband, dtype=np.float64)
+        kv = None if kidx is None else np.ascontiguousarray(kidx, dtype=np.int32)
+        call("sgpu_tpa_apply", self._h, C.c_void_p(in_dev), C.c_void_p(out_dev), int(nvec),
+             None if kv is None else _vp(kv), _vp(tb))
+
+    # ---- learned preconditioner
+    @staticmethod
+    def net_weight_count() -> int:
+        return _lib.lib().sgpu_net_weight_count()
+
+    def net_set_weights(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        if w.size != self.net_weight_count():
+            raise ValueError(f"need {self.net_weight_count()} weights")
+        call("sgpu_net_set_weights", self._h, _vp(w))
+
+    def net_get_weights(self):
+        w = np.empty(self.net_weight_count(), np.float32)
+        call("sgpu_net_get_weights", self._h, _vp(w))
+        return w
+
+    def net_apply(self, in_dev: int, out_dev: int, nvec: int):
+        call("sgpu_net_apply", self._h, C.c_void_p(in_dev), C.c_void_p(out_dev), int(nvec))
+
+    def net_grad(self, g_dev: int, t_dev: int, nvec: int):
+        grad = np.empty(self.net_weight_count(), np.float32)
+        loss = C.c_double()
+        call("sgpu_net_grad", self._h, C.c_void_p(g_dev), C.c_void_p(t_dev), int(nvec), _vp(grad), C.byref(loss))
+        return grad, loss.value
+
+    def net_train_step(self, g_dev: int, t_dev: int, nvec: int, lr: float) -> float:
+        loss = C.c_double()
+        call("sgpu_net_train_step", self._h, C.c_void_p(g_dev), C.c_void_p(t_dev), int(nvec), C.c_float(lr),
+             C.byref(loss))
+        return loss.value
+
     # ---- reductions
     def psi_rho_RT(self):
         rho = np.empty(self.sysm.NL)

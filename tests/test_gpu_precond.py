@@ -1,0 +1,132 @@
+"""Ground-state CG preconditioners on the GPU against the CPU oracle
+(oracle/net_oracle.py), and what they gain over the reference's plain CG.
+
+Tolerances: TPA (FP64 FFTs) 1e-11 relative; the network (BF16 activations,
+FP32 accumulation) 2e-2 relative to the largest output / gradient element,
+against an oracle that rounds the same tensors to BF16."""
+import numpy as np
+import pytest
+
+from oracle import net_oracle as N
+from salmon_b200 import precond as P, system as S
+
+pytestmark = pytest.mark.gpu
+
+SI8 = dict(ncell=(1, 1, 1), grid=(16, 16, 16), nkgrid=(2, 1, 1), Nb=12)
+NCONV = 8  # bands that must converge; the other 4 are buffer bands
+
+
+def _gpu(sysm, kAc, vloc, zu=None):
+    from salmon_b200.rt import GpuSystem
+    g = GpuSystem(sysm, "c128")
+    g.set_vloc(vloc)
+    g.update_projector(kAc)
+    if zu is not None:
+        g.gs_set_state(zu)
+    g.set_cg_delta(1e-24)  # the reference's 1e-15 stops CG before residuals reach 1e-8
+    return g
+
+
+def _coefs(sysm):
+    lap, nab = S.fd_coef()
+    d = sysm.desc()
+    lap3 = np.array([list(d.lapx), list(d.lapy), list(d.lapz)])
+    nab3 = np.array([list(d.nabx), list(d.naby), list(d.nabz)])
+    return lap3, nab3
+
+
+@pytest.mark.parametrize("shape", [(16, 16, 16), (8, 9, 12)])
+def test_tpa_matches_oracle(cuda_lib, shape):
+    import torch
+    if shape == (16, 16, 16):
+        sysm, kAc, vloc, _ = S.si_supercell_system(**SI8)
+    else:
+        sysm, kAc, vloc, _ = S.small_system(*shape, nk=2, nb=3)
+    rng = np.random.default_rng(5)
+    nv = sysm.nk_local
+    x = rng.standard_normal((nv, sysm.NL)) + 1j * rng.standard_normal((nv, sysm.NL))
+    tband = rng.uniform(0.2, 2.0, nv)
+    g = _gpu(sysm, kAc, vloc)
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.empty_like(xd)
+    g.tpa_apply(xd.data_ptr(), yd.data_ptr(), nv, tband, kidx=np.arange(nv)[::-1].copy())
+    y = yd.cpu().numpy()
+    g.close()
+    lap3, nab3 = _coefs(sysm)
+    for v in range(nv):
+        want = N.tpa_apply(x[v], shape, kAc[:, nv - 1 - v], tband[v], lap3, nab3)
+        assert np.abs(y[v] - want).max() <= 1e-11 * np.abs(want).max()
+
+
+def test_network_forward_and_gradient_match_oracle(cuda_lib):
+    import torch
+    sysm, kAc, vloc, _ = S.si_supercell_system(**SI8)
+    shape = (sysm.NLx, sysm.NLy, sysm.NLz)
+    rng = np.random.default_rng(6)
+    nv = 3
+    x = rng.standard_normal((nv, sysm.NL)) + 1j * rng.standard_normal((nv, sysm.NL))
+    t = rng.standard_normal((nv, sysm.NL)) + 1j * rng.standard_normal((nv, sysm.NL))
+    w = N.identity_weights(noise=0.2, seed=2)
+    g = _gpu(sysm, kAc, vloc)
+    g.net_set_weights(w)
+    np.testing.assert_array_equal(g.net_get_weights(), w)
+    xd, td = torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda()
+    yd = torch.empty_like(xd)
+    g.net_apply(xd.data_ptr(), yd.data_ptr(), nv)
+    y = yd.cpu().numpy()
+    grad, loss = g.net_grad(xd.data_ptr(), td.data_ptr(), nv)
+    g.close()
+    for v in range(nv):
+        want = N.forward(x[v], shape, w)[0]
+        assert np.abs(y[v] - want).max() <= 2e-2 * np.abs(want).max()
+    loss_o, grad_o = N.loss_grad(list(x), list(t), shape, w)
+    assert abs(loss - loss_o) <= 2e-2 * abs(loss_o)
+    for a, b in ((0, N.NW1), (N.NW1, N.NW1 + N.NW2), (N.NW1 + N.NW2, N.NET_NW)):
+        assert np.abs(grad[a:b] - grad_o[a:b]).max() <= 2e-2 * np.abs(grad_o[a:b]).max()
+
+
+def test_tpa_cg_converges_to_plain_cg_eigenvalues_in_fewer_iterations(cuda_lib):
+    sysm, kAc, vloc, zu = S.si_supercell_system(**SI8)
+    runs = {}
+    for kind in ("plain", "tpa"):
+        g = _gpu(sysm, kAc, vloc, zu)
+        g.set_cg_preconditioner(kind)
+        runs[kind] = P.solve_to(g, tol=1e-8, ncg=4, max_outer=300, nconv=NCONV)
+        g.close()
+    print({k: (v["outer"], v["cg_iterations"], v["residual"]) for k, v in runs.items()})
+    # plain CG need not reach 1e-8 within the budget; its eigenvalues are still
+    # good to ~ residual^2, far below the tolerance
+    assert runs["tpa"]["converged"] and runs["plain"]["residual"] < 1e-5
+    np.testing.assert_allclose(runs["tpa"]["esp"][:, :NCONV], runs["plain"]["esp"][:, :NCONV], atol=1e-9)
+    assert runs["tpa"]["cg_iterations"] < 0.7 * runs["plain"]["cg_iterations"]
+
+
+def test_learned_preconditioner_trains_and_cuts_cg_iterations(cuda_lib):
+    base = dict(SI8)
+    # training data: plain CG on one displaced configuration
+    sysm, kAc, vloc, zu = P.displaced_system(base, 0.05, seed=11)
+    g = _gpu(sysm, kAc, vloc, zu)
+    R, E, kidx, tband = P.cg_training_pairs(g, sysm, NCONV)
+    g.net_set_weights(N.identity_weights(noise=1e-2, seed=0))
+    hist = P.train(g, P.tpa_inputs(g, R, kidx, tband), E, steps=400, batch=16, lr=2e-3)
+    w = g.net_get_weights()
+    g.close()
+    print("loss", np.mean(hist[:5]), "->", np.mean(hist[-20:]))
+    assert np.mean(hist[-20:]) < 0.7 * np.mean(hist[:5])  # the network starts as TPA and fits the corrections
+    # evaluation: another displaced configuration, converged to 1e-8
+    sysm, kAc, vloc, zu = P.displaced_system(base, 0.05, seed=12)
+    runs = {}
+    for kind in ("plain", "tpa", "learned"):
+        g = _gpu(sysm, kAc, vloc, zu)
+        if kind == "learned":
+            g.net_set_weights(w)
+        g.set_cg_preconditioner(kind)
+        runs[kind] = P.solve_to(g, tol=1e-8, ncg=4, max_outer=300, nconv=NCONV)
+        g.close()
+    print({k: (v["outer"], v["cg_iterations"], v["residual"]) for k, v in runs.items()})
+    assert runs["learned"]["converged"] and runs["plain"]["residual"] < 1e-5
+    np.testing.assert_allclose(runs["learned"]["esp"][:, :NCONV], runs["plain"]["esp"][:, :NCONV], atol=1e-9)
+    # the gain over CG without the network: >= 30% fewer CG iterations to 1e-8
+    assert runs["learned"]["cg_iterations"] < 0.7 * runs["plain"]["cg_iterations"]
+    # and no worse than its fallback, TPA alone, by more than a quarter
+    assert runs["learned"]["cg_iterations"] < 1.25 * runs["tpa"]["cg_iterations"]
