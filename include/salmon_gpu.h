@@ -136,6 +136,23 @@ void* sgpu_state_ptr(sgpu_handle h);
 /* HOST Vloc(NL) -> device.  Vloc = Vh + Vpsl + Vexc (RT/dt_evolve.f90:206). */
 int sgpu_set_vloc(sgpu_handle h, const double* vloc);
 
+/* HOST Vpsl(NL) -> device: the local pseudopotential that sgpu_update_vloc
+ * adds (prep_ps.f90 Vpsl). */
+int sgpu_set_vpsl(sgpu_handle h, const double* vpsl);
+
+/* The self-consistent local potential of RT/dt_evolve.f90:190-207:
+ * Vloc = Vh[rho] + Vpsl + Vexc[rho] on the device, with Vh from the Poisson
+ * equation in reciprocal space (Hartree, common/Hartree.f90:20-130) and Vexc
+ * from the Perdew-Zunger LDA (exc_cor_pz, xc/builtin_pz.f90:23-80).  rho is
+ * HOST (NL), e.g. after the allreduce of sgpu_psi_rho's rho_l over k-ranks;
+ * NULL uses the density of the handle's resident orbitals.  eh_exc (HOST [2],
+ * may be NULL) receives the Hartree energy 1/2 sum Vh rho Hxyz and the
+ * exchange-correlation energy sum exc rho Hxyz.  Grid sizes must be 2^a 3^b <= 96. */
+int sgpu_update_vloc(sgpu_handle h, const double* rho, double* eh_exc);
+
+/* device -> HOST Vloc(NL) (FP64). */
+int sgpu_get_vloc(sgpu_handle h, double* vloc);
+
 /* ---- hot path ------------------------------------------------------------ */
 
 /* Sets k+A(t) for the following hpsi/hamiltonian calls and rebuilds the

@@ -27,6 +27,9 @@ ABI = {
     "sgpu_get_state": (C.c_int, [_vp, _vp]),
     "sgpu_state_ptr": (C.c_void_p, [_vp]),
     "sgpu_set_vloc": (C.c_int, [_vp, _vp]),
+    "sgpu_set_vpsl": (C.c_int, [_vp, _vp]),
+    "sgpu_update_vloc": (C.c_int, [_vp, _vp, _vp]),
+    "sgpu_get_vloc": (C.c_int, [_vp, _vp]),
     "sgpu_update_projector": (C.c_int, [_vp, _vp]),
     "sgpu_hamiltonian": (C.c_int, [_vp, C.c_double, _ip]),
     "sgpu_hpsi": (C.c_int, [_vp, _ip, _vp, _vp, _vp]),

@@ -372,7 +372,7 @@ int sgpu_destroy(sgpu_handle h) {
                   s->U, s->Uw, s->red, s->stage};
   for (void* p : bufs) cudaFree(p);
   void* gbufs[] = {s->gs_zu, s->gs_aux, s->gs_W, s->gs_st, s->gs_part, s->gs_A, s->gs_V, s->gs_w, s->gs_sweeps,
-                   s->occ_gs, s->gs_out, s->gs_res, s->gs_tb};
+                   s->occ_gs, s->gs_out, s->gs_res, s->gs_tb, s->vpsl, s->rho_d, s->exc_d};
   for (void* p : gbufs) cudaFree(p);
   if (s->gs_h) cudaFreeHost(s->gs_h);
   if (s->red_h) cudaFreeHost(s->red_h);
@@ -767,6 +767,47 @@ int sgpu_cg(sgpu_handle h, int ncg, double* esp_var, int* iters) {
   }
   if ((rc = gs_copy_out(s, s->gs_out, esp_var))) return rc;
   if (iters) std::memcpy(iters, it_all.data(), it_all.size() * sizeof(int));
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int sgpu_set_vpsl(sgpu_handle h, const double* vpsl) {
+  if (!valid(h) || !vpsl) return fail(SGPU_ERR_ARG, "sgpu_set_vpsl: null argument");
+  System* s = h;
+  if (!s->vpsl) {
+    CK(cudaMalloc(&s->vpsl, (size_t)s->NL * sizeof(double)));
+    CK(cudaMalloc(&s->rho_d, (size_t)s->NL * sizeof(double)));
+    CK(cudaMalloc(&s->exc_d, 2 * sizeof(double)));
+  }
+  CK(cudaMemcpyAsync(s->vpsl, vpsl, (size_t)s->NL * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int sgpu_update_vloc(sgpu_handle h, const double* rho, double* eh_exc) {
+  if (!valid(h)) return fail(SGPU_ERR_ARG, "null handle");
+  System* s = h;
+  if (!s->vpsl) return fail(SGPU_ERR_STATE, "sgpu_update_vloc: call sgpu_set_vpsl first");
+  if (!(sgpu::fft_size_ok(s->NLx) && sgpu::fft_size_ok(s->NLy) && sgpu::fft_size_ok(s->NLz)))
+    return fail(SGPU_ERR_UNSUPPORTED, "sgpu_update_vloc: grid sizes must be 2^a 3^b <= 96");
+  if (rho) {
+    CK(cudaMemcpyAsync(s->rho_d, rho, (size_t)s->NL * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  } else {
+    if (!s->have_state) return fail(SGPU_ERR_STATE, "sgpu_update_vloc: no state loaded");
+    CK(sgpu::launch_psi_rho(*s, s->rho_d));
+  }
+  CK(sgpu::launch_update_vloc(*s, s->rho_d, s->exc_d));
+  if (eh_exc) CK(cudaMemcpyAsync(eh_exc, s->exc_d, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  s->have_vloc = true;
+  return 0;
+}
+
+int sgpu_get_vloc(sgpu_handle h, double* vloc) {
+  if (!valid(h) || !vloc) return fail(SGPU_ERR_ARG, "sgpu_get_vloc: null argument");
+  System* s = h;
+  if (!s->have_vloc) return fail(SGPU_ERR_STATE, "sgpu_get_vloc: no Vloc set");
+  CK(cudaMemcpyAsync(vloc, s->vloc64, (size_t)s->NL * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   return 0;
 }

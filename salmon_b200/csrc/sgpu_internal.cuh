@@ -170,6 +170,9 @@ struct System {
   bool net_ready = false;          // a preconditioner network has been loaded
   void* net = nullptr;             // its weights, optimiser state and workspace (k_net.cu)
   double* gs_tb = nullptr;         // [nkl] kinetic energy of the band in CG (TPA)
+  double* vpsl = nullptr;          // [NL] local pseudopotential (for the self-consistent Vloc)
+  double* rho_d = nullptr;         // [NL] density used by the last potential update
+  double* exc_d = nullptr;         // [2] Hartree and exchange-correlation energies
   double* gs_res = nullptr;        // [nkl][NB] residual norms of the last sgpu_cg
 };
 
@@ -242,6 +245,9 @@ cudaError_t launch_cg_dir(const System& s, const double2* zu, double2* W, void* 
 bool fft_size_ok(int n);
 // The learned preconditioner applied in place to nvec vectors (k_net.cu).
 cudaError_t launch_precond_net(const System& s, double2* data, int nvec);
+// Vloc = Vh[rho] + Vpsl + Vxc[rho] into vloc64/vloc32 (k_xc.cu); energies_dev[2] =
+// (Eh, Exc).  Grid sizes 2^a 3^b <= 96.
+cudaError_t launch_update_vloc(const System& s, const double* rho_dev, double* energies_dev);
 void net_free(System& s);
 cudaError_t launch_fft3d(const System& s, double2* data, int nvec, int sign, bool normalise);
 cudaError_t launch_tpa(const System& s, double2* data, int nvec, const double* tband_dev, int vecs_per_k,

@@ -1,14 +1,18 @@
 """Ground-state and real-time drivers over the C ABI.
 
-These follow the control flow of SALMON's ARTED drivers with the potential
-held fixed (no Hartree / exchange-correlation update between steps):
+These follow the control flow of SALMON's ARTED drivers, either with the
+local potential held fixed or updated self-consistently (Hartree + PZ LDA on
+the device, sgpu_update_vloc):
 
   init_Ac          RT/init_Ac.f90:17-100      A_ext(t) of 'impulse' and 'Acos<n>' pulses
   ground_state     control/ground_state.f90:100-150  Gram-Schmidt, subspace diag,
                                               Gram-Schmidt, CG, Gram-Schmidt per iteration
-  rt_propagate     control/control_sc.f90:150-230 with dt_evolve_KB 'middlepoint'
-                   (RT/dt_evolve.f90:45-49): k+A at the midpoint for the Taylor step,
-                   k+A(t+dt) for the current
+  rt_propagate     control/control_sc.f90:150-230 with dt_evolve_omp_KB
+                   'middlepoint' (RT/dt_evolve.f90:45-49, 176-207): k+A at the
+                   midpoint for the Taylor step, then rho -> Vh + Vexc -> Vloc
+                   (scf=True), k+A(t+dt) for the current
+  ground_state_scf the ground-state loop with the density mixed linearly between
+                   iterations (the reference mixes with Broyden, common/broyden.f90)
 """
 from __future__ import annotations
 
@@ -56,6 +60,33 @@ def ground_state(g, n_iter: int = 4, ncg: int = 4):
     return esp, esp_var, history
 
 
+def ground_state_scf(g, n_iter: int = 40, ncg: int = 4, mix: float = 0.3):
+    """Ground-state iterations with a self-consistent Vloc = Vh + Vpsl + Vexc
+    (the caller has set Vpsl and an initial Vloc).  After each iteration the
+    occupied bands' density rho_out is mixed into rho_in <- (1-mix) rho_in + mix
+    rho_out and the potential is rebuilt from rho_in.  Returns (esp, history)
+    with history[i] = (sum of esp, max esp_var, |rho_out - rho_in| Hxyz)."""
+    history = []
+    rho_in = None
+    esp = None
+    for _ in range(n_iter):
+        g.gram_schmidt()
+        esp = g.subspace_diag()
+        g.gram_schmidt()
+        esp_var, _ = g.cg(ncg)
+        g.gram_schmidt()
+        g.gs_to_rt()
+        rho_out = g.psi_rho_RT()
+        if rho_in is None:
+            rho_in = rho_out
+        drho = float(np.abs(rho_out - rho_in).sum() * g.sysm.Hxyz)
+        rho_in = (1 - mix) * rho_in + mix * rho_out
+        g.update_vloc(rho_in)
+        history.append((float(esp.sum()), float(esp_var.max()), drho))
+    esp = g.subspace_diag()
+    return esp, history
+
+
 def band_energy(g, sysm, kAc, vloc):
     """Ekin + Enl + sum_i Vloc_i rho_i Hxyz of the resident orbitals (FP64)."""
     ek, en = g.energy_terms(kAc)
@@ -63,25 +94,45 @@ def band_energy(g, sysm, kAc, vloc):
     return ek + en + float(np.dot(vloc, rho)) * sysm.Hxyz
 
 
-def rt_propagate(g, sysm, kAc0, vloc, Ac, dt: float, Nt: int, energy_every: int = 0):
+def total_energy(g, sysm, kAc, vpsl):
+    """Ekin + Enl + sum Vpsl rho Hxyz + Eh + Exc of the resident orbitals (FP64;
+    the ion-ion term is a constant and left out); also rebuilds Vloc from their
+    density, as the reference's step does."""
+    ek, en = g.energy_terms(kAc)
+    rho = g.psi_rho_RT()
+    eh, exc = g.update_vloc(rho)
+    return ek + en + float(np.dot(vpsl, rho)) * sysm.Hxyz + eh + exc
+
+
+def rt_propagate(g, sysm, kAc0, vloc, Ac, dt: float, Nt: int, energy_every: int = 0, scf: bool = False):
     """Nt middle-point Taylor steps of the resident orbitals; returns
     (javt (Nt+1,3) with javt[0] the current before the first step,
-     energies {step: band energy} every `energy_every` steps)."""
+     energies {step: energy} every `energy_every` steps).
+    scf=False: vloc is the fixed local potential (energies: band energy).
+    scf=True: vloc is Vpsl; Vloc = Vh + Vpsl + Vexc is rebuilt from the density
+    after every step on the device (energies: total_energy)."""
     kAc0 = np.ascontiguousarray(kAc0, dtype=np.float64)
-    g.set_vloc(vloc)
+    if scf:
+        g.set_vpsl(vloc)
+        g.update_vloc()
+    else:
+        g.set_vloc(vloc)
+    energy = (lambda k: total_energy(g, sysm, k, vloc)) if scf else (lambda k: band_energy(g, sysm, k, vloc))
     javt = np.zeros((Nt + 1, 3))
     javt[0] = g.current_RT(kAc0 + Ac[1][:, None])
     energies = {}
     if energy_every:
-        energies[0] = band_energy(g, sysm, kAc0 + Ac[1][:, None], vloc)
+        energies[0] = energy(kAc0 + Ac[1][:, None])
     for it in range(Nt):
         kmid = kAc0 + 0.5 * (Ac[it + 1] + Ac[it + 2])[:, None]   # kAc0 + (Ac(it)+Ac(it+1))/2
         g.update_projector(kmid)
         g.hamiltonian(dt)
+        if scf:
+            g.update_vloc()       # psi_rho_RT, Hartree, Exc_Cor, Vloc (dt_evolve.f90:190-207)
         knew = kAc0 + Ac[it + 2][:, None]
         javt[it + 1] = g.current_RT(knew)
         if energy_every and (it + 1) % energy_every == 0:
-            energies[it + 1] = band_energy(g, sysm, knew, vloc)
+            energies[it + 1] = energy(knew)
     return javt, energies
 
 

@@ -97,6 +97,23 @@ class GpuSystem:
         call("sgpu_set_vloc", self._h, _vp(v))
 
     # ---- hot path
+    def set_vpsl(self, vpsl):
+        v = np.ascontiguousarray(vpsl, dtype=np.float64)
+        call("sgpu_set_vpsl", self._h, _vp(v))
+
+    def update_vloc(self, rho=None):
+        """Vloc = Vh[rho] + Vpsl + Vexc[rho] on the device (Hartree + PZ LDA);
+        rho defaults to the resident orbitals' density.  Returns (Eh, Exc)."""
+        e = np.zeros(2)
+        r = None if rho is None else np.ascontiguousarray(rho, dtype=np.float64)
+        call("sgpu_update_vloc", self._h, None if r is None else _vp(r), _vp(e))
+        return float(e[0]), float(e[1])
+
+    def get_vloc(self):
+        v = np.empty(self.sysm.NL)
+        call("sgpu_get_vloc", self._h, _vp(v))
+        return v
+
     def update_projector(self, kAc):
         k = np.ascontiguousarray(kAc, dtype=np.float64)
         if k.shape != (3, self.sysm.NK):

@@ -373,11 +373,12 @@ def microbench_system(N: int, nkgrid=(4, 4, 4), Nb: int = 32, A=(1e-2, 0.0, 0.0)
 
 
 def si_supercell_system(ncell=(1, 1, 1), grid=(16, 16, 16), nkgrid=(4, 4, 4), Nb: int = 16, A=(0.0, 0.0, 0.0),
-                        a: float = 10.26, seed: int = SEED, with_orbitals: bool = True):
+                        a: float = 10.26, seed: int = SEED, with_orbitals: bool = True, Nocc: int | None = None):
     """Diamond-Si supercell of ncell cubic 8-atom cells (a = 10.26 bohr) on the
     given grid: 8*prod(ncell) atoms x {s,px,py,pz} Gaussian projectors (r_c =
     R_ps = 2 bohr), V_loc = seeded periodic Gaussians on the atoms, uniform
-    nkgrid k-points, Nb bands.  The shapes of the Si8 / Si16 / Si64 systems:
+    nkgrid k-points, Nb bands of which the lowest Nocc (default all) are occupied
+    (2/NK each) and propagated in real time.  The shapes of the Si8 / Si16 / Si64 systems:
     ncell (1,1,1) 16^3, (1,1,2) 16x16x32, (2,2,2) 32^3.
     Returns (system, kAc (3,NK), Vloc (NL,), zu (nk,Nb,NL) complex128 or None)."""
     rng = np.random.default_rng(seed)
@@ -387,7 +388,9 @@ def si_supercell_system(ncell=(1, 1, 1), grid=(16, 16, 16), nkgrid=(4, 4, 4), Nb
     bl = 2 * np.pi / aL
     kAc0 = uniform_k_grid(*nkgrid, bl)
     NK = kAc0.shape[1]
-    occ = np.full((NK, Nb), 2.0 / NK)
+    Nocc = Nb if Nocc is None else Nocc
+    occ = np.zeros((NK, Nb))
+    occ[:, :Nocc] = 2.0 / NK
     cells = np.array([[i, j, k] for i in range(nc[0]) for j in range(nc[1]) for k in range(nc[2])])
     Rion = np.concatenate([(DIAMOND_RED + c) * a for c in cells])
     Mps, Jxyz, Jxx, Jyy, Jzz, dist = calc_jxyz(NLx, NLy, NLz, aL, Rion, 2.0)
@@ -396,7 +399,7 @@ def si_supercell_system(ncell=(1, 1, 1), grid=(16, 16, 16), nkgrid=(4, 4, 4), Nb
     depth = rng.uniform(0.5, 2.0, Rion.shape[0])
     width = rng.uniform(1.0, 2.0, Rion.shape[0])
     vloc = periodic_gaussian_vloc(NLx, NLy, NLz, aL, Rion, depth, width)
-    sysm = System(NLx=NLx, NLy=NLy, NLz=NLz, aL=aL, kAc0=kAc0, NB=Nb, NBoccmax=Nb, occ=occ, Rion=Rion, Rps=2.0,
+    sysm = System(NLx=NLx, NLy=NLy, NLz=NLz, aL=aL, kAc0=kAc0, NB=Nb, NBoccmax=Nocc, occ=occ, Rion=Rion, Rps=2.0,
                   Mps=Mps, Jxyz=Jxyz, Jxx=Jxx, Jyy=Jyy, Jzz=Jzz, uV=uV, iuV=iuV, a_tbl=a_tbl)
     sysm.extra.update(seed=seed, depth=depth, width=width)
     kAc = np.ascontiguousarray(kAc0 + np.asarray(A, dtype=np.float64)[:, None])

@@ -1,0 +1,33 @@
+"""CPU checks of the self-consistent-potential oracle (oracle/scf_oracle.py)."""
+import numpy as np
+
+from oracle import scf_oracle as X
+
+
+def test_hartree_of_a_plane_wave_density():
+    shape, aL = (8, 12, 16), np.array([5.0, 6.0, 7.0])
+    x = np.arange(8)[:, None, None] * aL[0] / 8
+    y = np.arange(12)[None, :, None] * aL[1] / 12
+    g = np.array([2 * np.pi / aL[0] * 1, 2 * np.pi / aL[1] * 2, 0.0])
+    rho = np.broadcast_to(0.3 + np.cos(g[0] * x + g[1] * y), shape).ravel()
+    vh = X.hartree(rho, shape, aL)
+    want = (4 * np.pi / (g @ g) * np.cos(g[0] * x + g[1] * y) * np.ones(shape)).ravel()
+    np.testing.assert_allclose(vh, want, atol=1e-12 * np.abs(want).max())
+
+
+def test_pz_exchange_and_correlation_values():
+    # rs = 1 and rs = 2 from the PZ formulas (exchange -0.458165/rs; correlation fits)
+    for rs, ec in ((1.0 - 1e-12, 0.0311 * np.log(1 - 1e-12) - 0.048 + 0.002 * (1 - 1e-12) * np.log(1 - 1e-12) - 0.0116 * (1 - 1e-12)),
+                   (2.0, -0.1423 / (1 + 1.0529 * np.sqrt(2.0) + 0.3334 * 2.0))):
+        rho = 3.0 / (4 * np.pi * rs ** 3) - 1e-10
+        e, _ = X.pz(np.array([rho]))
+        assert abs(e[0] - (-0.4581652932831429 / rs + ec)) < 1e-9
+
+
+def test_pz_potential_is_the_density_derivative():
+    rho = np.array([1e-3, 2e-2, 0.1, 0.5, 2.0])
+    e, v = X.pz(rho)
+    h = 1e-7 * rho
+    ep, _ = X.pz(rho + h)
+    em, _ = X.pz(rho - h)
+    np.testing.assert_allclose(v, ((rho + h) * ep - (rho - h) * em) / (2 * h), rtol=1e-6)
