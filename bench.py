@@ -120,10 +120,18 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
-def make_workload(args, rank):
-    from salmon_b200 import system as S
+def make_workload(args, rank, world=1):
+    """The microbench system on a k-grid of nkgrid x nkgrid x (nkgrid * world)
+    points, sharded over the ranks by the reference's k partition (each rank
+    gets nkgrid^3 k-points: weak scaling); the orbitals of the rank's block only."""
+    from salmon_b200 import dist as D, system as S
     nk = args.nkgrid
-    return S.microbench_system(args.grid, nkgrid=(nk, nk, nk), Nb=args.nb, seed=S.SEED + rank)
+    sysm, kAc, vloc, _ = S.microbench_system(args.grid, nkgrid=(nk, nk, nk * world), Nb=args.nb, with_orbitals=False)
+    loc = D.local_system(sysm, rank, world)
+    rng = np.random.default_rng(S.SEED + rank)
+    shape = (loc.nk_local, args.nb, loc.NL)
+    zu = S.orthonormalise(rng.standard_normal(shape) + 1j * rng.standard_normal(shape), loc.Hxyz)
+    return loc, kAc, vloc, zu
 
 
 def cpu_baseline(sysm, kAc, vloc, zu, seconds):
@@ -302,7 +310,7 @@ def main():
     build.build()
     from salmon_b200.rt import GpuSystem
 
-    sysm, kAc, vloc, zu = make_workload(args, rank)
+    sysm, kAc, vloc, zu = make_workload(args, rank, world)
     norb = sysm.nk_local * sysm.NBoccmax
     NL = sysm.NL
     hbm_peak, peak_kind = measured_peaks()
@@ -375,11 +383,10 @@ def main():
             g.hamiltonian(DT)
             rho = g.psi_rho_RT()
             jav = g.current_RT(kt)
-            if world > 1:
-                import torch.distributed as dist
-                t = torch.from_numpy(np.concatenate([rho, jav])).cuda()
-                dist.all_reduce(t)
-                t.cpu()
+            if world > 1:  # comm_summation of rho and J (psi_rho.f90:88, current.f90:286) over NCCL
+                from salmon_b200 import dist as D
+                rho = D.comm_summation(rho)
+                jav = D.comm_summation(jav)
         e1.record(stream)
         e1.synchronize()
         ms_e2e = max_over_ranks(e0.elapsed_time(e1))
