@@ -350,7 +350,8 @@ enum {
   SGPU_KERNEL_TAYLOR_LAST = 1,  /* the fused last Taylor pass (H application + update), on workspace */
   SGPU_KERNEL_UVPSI = 2,        /* the Kleinman-Bylander projections of every resident orbital       */
   SGPU_KERNEL_PSI_RHO = 3,      /* the density reduction                                             */
-  SGPU_KERNEL_KB_FIELD = 4      /* the Kleinman-Bylander term at the sphere points from the projections */
+  SGPU_KERNEL_KB_FIELD = 4,     /* the Kleinman-Bylander term at the sphere points from the projections */
+  SGPU_KERNEL_KB_TERM = 5       /* projections and KB term in one kernel, as the Taylor step runs them  */
 };
 
 /* Launches `kernel` reps times back to back on the handle's stream between two

@@ -65,7 +65,7 @@ ABI = {
 
 PARAMS = {"nslab": 0, "launches": 1, "uvpsi_split": 2, "cg_precond": 3}
 
-KERNELS = {"stencil_pass": 0, "taylor_last": 1, "uvpsi": 2, "psi_rho": 3, "kb_field": 4}
+KERNELS = {"stencil_pass": 0, "taylor_last": 1, "uvpsi": 2, "psi_rho": 3, "kb_field": 4, "kb_term": 5}
 
 _LIB = None
 

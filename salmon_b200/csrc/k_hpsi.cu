@@ -279,6 +279,177 @@ static cudaError_t launch_kbfield_t(const System& s, int o_beg, int nb, int nbk,
   return cudaGetLastError();
 }
 
+// ------------------------------------------------ projections + KB field ---
+// One kernel for U and W of the points inside exactly one item (the KB term
+// of one H application): a CTA owns (band quad, item); its UM_SPLIT warps
+// first build the 8x8 projection tile over the atom's points (as k_uvpsi,
+// summed in warp order), keep U in shared memory (and store it for the
+// entry-wise kernel of multi-item points), then sweep the atom's points again
+// for W = zproj U (as k_kbfield), so U never makes a round trip through global
+// memory between two launches.
+template <typename R, int UM_SPLIT>
+__global__ void __launch_bounds__(32 * UM_SPLIT) k_kb_fused(const C2<R>* __restrict__ in, int ld_in, int o_beg, int nb,
+                                                           int nbk, int kl0, int nquad_k,
+                                                           const double2* __restrict__ zproj, int Nlma, int Nps,
+                                                           const int* __restrict__ idx, const int* __restrict__ kbq,
+                                                           const int* __restrict__ atom_off,
+                                                           const int4* __restrict__ items,
+                                                           const int* __restrict__ lma_list, const int* __restrict__ iuV,
+                                                           double scale, double2* __restrict__ U, int nsp,
+                                                           C2<R>* __restrict__ W) {
+  __shared__ double2 part[UM_SPLIT][32];
+  __shared__ double2 Us[4][4];  // [projector][band of the quad]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int quad = blockIdx.x;
+  const int kq = quad / nquad_k;
+  const int kl = kl0 + kq;
+  const int b_first = kl * nbk + 4 * (quad - kq * nquad_k);
+  const int o_lo = max(o_beg, kl * nbk), o_hi = min(o_beg + nb, (kl + 1) * nbk);
+  const int4 item = items[blockIdx.y];
+  const int a = item.x, l0 = item.y, np = item.z;
+  const int p0 = atom_off[a], mps = atom_off[a + 1] - p0;
+  const int krow = lane & 3, n = lane >> 2;
+
+  // ---- phase 1: U tile (rows: Re/Im zproj of the item's projectors; columns: Re/Im of 4 bands)
+  {
+    const int ob = b_first + (n >> 1);
+    const bool bvalid = ob >= o_lo && ob < o_hi;
+    const C2<R>* src = in + (size_t)(bvalid ? ob - o_beg : 0) * ld_in;
+    const int bpart = n & 1;
+    const int pa = n & 3;
+    const bool avalid = pa < np;
+    const double* zrow =
+        reinterpret_cast<const double*>(zproj + ((size_t)kl * Nlma + (avalid ? lma_list[l0 + pa] : 0)) * Nps) + (n >> 2);
+    double c0 = 0.0, c1 = 0.0, e0 = 0.0, e1 = 0.0;
+    constexpr int PTS = 4 * UM_UNROLL;
+    constexpr int STRIDE = PTS * UM_SPLIT;
+    int j0 = warp * PTS;
+    int gl = j0 + lane < mps ? __ldg(idx + p0 + j0 + lane) : 0;
+    for (; j0 < mps; j0 += STRIDE) {
+      const int jn = j0 + STRIDE;
+      const int nl = jn + lane < mps ? __ldg(idx + p0 + jn + lane) : 0;
+      double av[UM_UNROLL], bv[UM_UNROLL];
+#pragma unroll
+      for (int u = 0; u < UM_UNROLL; ++u) {
+        const int j = j0 + 4 * u + krow;
+        const int g = __shfl_sync(0xffffffffu, gl, 4 * u + krow);
+        av[u] = 0.0;
+        bv[u] = 0.0;
+        if (j < mps) {
+          if (avalid) av[u] = __ldg(zrow + 2 * (size_t)j);
+          if (bvalid) {
+            const C2<R> v = src[g];
+            bv[u] = bpart ? (double)v.y : (double)v.x;
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < UM_UNROLL; u += 2) {
+        mma_f64_8x8x4(c0, c1, av[u], bv[u]);
+        mma_f64_8x8x4(e0, e1, av[u + 1], bv[u + 1]);
+      }
+      gl = nl;
+    }
+    part[warp][lane] = make_double2(c0 + e0, c1 + e1);
+  }
+  __syncthreads();
+  if (warp == 0) {
+    double2 t = part[0][lane];
+#pragma unroll
+    for (int w = 1; w < UM_SPLIT; ++w) {
+      t.x += part[w][lane].x;
+      t.y += part[w][lane].y;
+    }
+    const double d0 = __shfl_down_sync(0xffffffffu, t.x, 16);
+    const double d1 = __shfl_down_sync(0xffffffffu, t.y, 16);
+    if (lane < 16) {
+      const int p = lane >> 2, bq = lane & 3, o = b_first + bq;
+      double2 u = make_double2(0.0, 0.0);
+      if (p < np && o >= o_lo && o < o_hi) {
+        const int ilma = lma_list[l0 + p];
+        const double f = scale * (double)iuV[ilma];
+        u = make_double2((t.x + d1) * f, (t.y - d0) * f);
+        U[(size_t)(o - o_beg) * Nlma + ilma] = u;
+      }
+      Us[p][bq] = u;
+    }
+  }
+  __syncthreads();
+
+  // ---- phase 2: W at the atom's single-item points, 8 points per pair of MMAs
+  {
+    const int p = krow;  // B row / A column: projector
+    const double2 u = Us[p][n >> 1];
+    const double bre = (n & 1) ? u.y : u.x;   // rows of Re zproj
+    const double bim = (n & 1) ? u.x : -u.y;  // rows of Im zproj
+    const double2* zp = zproj + ((size_t)kl * Nlma + (p < np ? lma_list[l0 + p] : 0)) * Nps;
+    const int oc = b_first + p;  // the orbital of this lane's C elements (C column pair 2p, 2p+1)
+    const bool cvalid = oc >= o_lo && oc < o_hi;
+    C2<R>* Wb = W + (size_t)(cvalid ? oc - o_beg : 0) * nsp;
+    constexpr int T = 8;
+    for (int j0 = warp * 8 * T; j0 < mps; j0 += UM_SPLIT * 8 * T) {
+      double2 z[T];
+      int q[T];
+#pragma unroll
+      for (int t = 0; t < T; ++t) {
+        const int j = j0 + 8 * t + n;
+        z[t] = make_double2(0.0, 0.0);
+        q[t] = -1;
+        if (j < mps) {
+          if (p < np) z[t] = __ldg(zp + j);
+          q[t] = __ldg(kbq + p0 + j);
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < T; ++t) {
+        double c0 = 0.0, c1 = 0.0;
+        mma_f64_8x8x4(c0, c1, z[t].x, bre);
+        mma_f64_8x8x4(c0, c1, z[t].y, bim);
+        if (cvalid && q[t] >= 0) Wb[q[t]] = mk<R>((R)c0, (R)c1);
+      }
+    }
+  }
+}
+
+template <typename R, int SPLIT>
+static cudaError_t launch_kb_fused_split(const System& s, const void* in, int ld_in, const int* idx, int o_beg, int nb,
+                                         int nbk, void* W) {
+  const int kl0 = o_beg / nbk, kl1 = (o_beg + nb - 1) / nbk;
+  const int nquad_k = (nbk + 3) / 4;
+  const int nquad = (kl1 - kl0 + 1) * nquad_k;
+  dim3 grid(nquad, s.nitems);
+  k_kb_fused<R, SPLIT><<<grid, 32 * SPLIT, 0, s.launch_stream()>>>(
+      (const C2<R>*)in, ld_in, o_beg, nb, nbk, kl0, nquad_k, s.zproj64, s.Nlma, s.Nps, idx, s.kbq, s.atom_off, s.items,
+      s.lma_list, s.iuV_d, s.Hxyz, s.U, s.nsp, (C2<R>*)W);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || s.n_multi == 0) return e;
+  dim3 g2((s.n_multi + 255) / 256, (nb + KU - 1) / KU);
+  k_kbfield_multi<R><<<g2, 256, 0, s.launch_stream()>>>(s.U, nb, o_beg, nbk, s.zproj64, s.Nlma, s.Nps, s.rec, s.cont,
+                                                         s.kb_multi, s.n_multi, s.nsp, (C2<R>*)W);
+  return cudaGetLastError();
+}
+
+template <typename R>
+static cudaError_t launch_kb_fused_t(const System& s, const void* in, int ld_in, const int* idx, int o_beg, int nb,
+                                     int nbk, void* W) {
+  switch (s.um_split) {
+    case 1: return launch_kb_fused_split<R, 1>(s, in, ld_in, idx, o_beg, nb, nbk, W);
+    case 2: return launch_kb_fused_split<R, 2>(s, in, ld_in, idx, o_beg, nb, nbk, W);
+    case 8: return launch_kb_fused_split<R, 8>(s, in, ld_in, idx, o_beg, nb, nbk, W);
+    default: return launch_kb_fused_split<R, 4>(s, in, ld_in, idx, o_beg, nb, nbk, W);
+  }
+}
+
+cudaError_t launch_kb_term(const System& s, const void* in, bool from_S, int o_beg, int nb, int nbk, void* W,
+                           int prec) {
+  if (s.Nlma == 0 || nb == 0) return cudaSuccess;
+  const void* src = from_S ? s.Sbuf : in;
+  const int ld = from_S ? s.nsp : s.NL;
+  const int* idx = from_S ? s.qmap : s.idx_proj;
+  if ((prec < 0 ? s.prec : prec) == SGPU_PREC_C64) return launch_kb_fused_t<float>(s, src, ld, idx, o_beg, nb, nbk, W);
+  return launch_kb_fused_t<double>(s, src, ld, idx, o_beg, nb, nbk, W);
+}
+
 cudaError_t launch_kbfield(const System& s, int o_beg, int nb, int nbk, void* W, int prec) {
   if (s.nsp == 0 || nb == 0) return cudaSuccess;
   if ((prec < 0 ? s.prec : prec) == SGPU_PREC_C64) return launch_kbfield_t<float>(s, o_beg, nb, nbk, W);

@@ -82,13 +82,8 @@ int one_orbital_k(const System* s, int ik) { return (ik - s->NK_s) * s->NBocc; }
 // points, then the stencil pass (which may export its output to S).
 cudaError_t apply_h(System* s, int mode, sgpu::PassIO io, int o_beg, int nb, int nbk, int prec, bool u_from_S) {
   cudaError_t e;
-  if (u_from_S)
-    e = sgpu::launch_uvpsi_from_S(*s, s->Sbuf, o_beg, nb, nbk, true);
-  else
-    e = sgpu::launch_uvpsi(*s, io.in, o_beg, nb, nbk, true, prec);
-  if (e != cudaSuccess) return e;
   if (s->nsp > 0) {
-    if ((e = sgpu::launch_kbfield(*s, o_beg, nb, nbk, s->Wbuf, prec)) != cudaSuccess) return e;
+    if ((e = sgpu::launch_kb_term(*s, io.in, u_from_S, o_beg, nb, nbk, s->Wbuf, prec)) != cudaSuccess) return e;
     io.W = s->Wbuf;
   }
   return sgpu::launch_hpsi_pass(*s, mode, io, o_beg, nb, nbk, prec);
@@ -600,6 +595,8 @@ int sgpu_time_kernel(sgpu_handle h, int kernel, int reps, double* ms_per_launch)
         return sgpu::launch_uvpsi_from_S(*s, s->Sbuf, 0, s->norb, s->NBocc, true);
       case SGPU_KERNEL_PSI_RHO:
         return sgpu::launch_psi_rho(*s, (double*)s->stage);
+      case SGPU_KERNEL_KB_TERM:  // projections from S and the KB field in one kernel (as in the Taylor step)
+        return sgpu::launch_kb_term(*s, s->zu, true, 0, s->norb, s->NBocc, s->Wbuf);
       default:
         return cudaErrorInvalidValue;
     }

@@ -188,6 +188,11 @@ cudaError_t launch_uvpsi(const System& s, const void* in, int o_beg, int nb, int
 cudaError_t launch_uvpsi_from_S(const System& s, const void* S, int o_beg, int nb, int nbk, bool scale_iuv);
 // W[b][q] = sum_entries zproj U[b] at every sphere point (needs U of the batch)
 cudaError_t launch_kbfield(const System& s, int o_beg, int nb, int nbk, void* W, int prec = -1);
+// U and W of one H application in one kernel (plus the entry-wise kernel for
+// points in several projector items): projections from S (from_S, the sphere
+// values exported by the previous pass) or gathered from the orbitals `in`.
+cudaError_t launch_kb_term(const System& s, const void* in, bool from_S, int o_beg, int nb, int nbk, void* W,
+                           int prec = -1);
 // dynamic shared memory of the pass kernel
 size_t pass_smem_bytes(int prec, int NLy, int NLz, int maxpts, bool with_w, int NLx);
 

@@ -64,11 +64,11 @@ def test_batch_graph_matches_sequential_steps(cuda_lib, precision):
         g.close()
     for w, x in zip(want, got):
         assert _rel(x, w) <= TOL[precision]
-    # 3 kernels per H application, 4 per Taylor step, 2 x nsteps steps (+1 for
-    # the entry-wise KB field where spheres overlap)
-    assert counts[0] == 2 * nsteps * 4 * 3
-    assert counts[1] == 2 * nsteps * 4 * 3
-    assert counts[2] == 2 * nsteps * 4 * 4
+    # 2 kernels per H application (KB term, stencil pass), 4 per Taylor step,
+    # 2 x nsteps steps (+1 for the entry-wise KB field where spheres overlap)
+    assert counts[0] == 2 * nsteps * 4 * 2
+    assert counts[1] == 2 * nsteps * 4 * 2
+    assert counts[2] == 2 * nsteps * 4 * 3
 
 
 def test_batch_recaptures_on_new_dt(cuda_lib):
