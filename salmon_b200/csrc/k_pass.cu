@@ -47,6 +47,11 @@ struct PassArgs {
   // sp_off[x] .. sp_off[x+1]-1 (at most maxpts); lqi[i] is the index of grid
   // point i among its plane's sphere points, or -1.
   const int* sp_off;
+  // y-blocks (YB form, planes wider than one CTA): each orbital plane is split
+  // into nyblk CTAs of NYB rows; sp_blk[x*(nyblk+1) + yb] is the first sphere
+  // point of plane x in rows >= yb*NYB (sp_blk[x*(nyblk+1)] = sp_off[x]).
+  int NYB, nyblk;
+  const int* sp_blk;
   const short* lqi;
   const C2<R>* W;        // [nb][nsp] KB term at the sphere points (null: none)
   C2<R>* S;              // [nb][nsp] export of the output (null: none)
@@ -140,15 +145,20 @@ template <typename R> struct PassGeom {
   static constexpr int NR = std::is_same<R, float>::value ? 8 : 6;  // ring planes
 };
 
-size_t pass_smem_bytes(int prec, int NLy, int NLz, int maxpts, bool with_w, int NLx) {
+size_t pass_smem_bytes(int prec, int NLy, int NLz, int maxpts, bool with_w, int NLx, int nyblk, int NYB) {
   const size_t e = prec == SGPU_PREC_C64 ? sizeof(float2) : sizeof(double2);
   const int NR = prec == SGPU_PREC_C64 ? PassGeom<float>::NR : PassGeom<double>::NR;
-  return e * (size_t)NR * ((size_t)NLy * NLz + (with_w ? (size_t)maxpts : 0)) + sizeof(int) * (size_t)(NLx + 1);
+  const size_t ryz = nyblk > 1 ? (size_t)(NYB + 8) * NLz : (size_t)NLy * NLz;
+  return e * (size_t)NR * (ryz + (with_w ? (size_t)maxpts : 0)) + sizeof(int) * (size_t)NLx * (nyblk + 1) +
+         sizeof(int);
 }
 
 // MODE 0: out = H in.   MODE 1: also tt = H in - V in before the nonlocal term.
 // MODE 2: zu = zu + zf0 t1 + zf1 t2 + zf2 in + zf3 H in   (RT/hamiltonian.f90:99-122).
-template <typename R, int RZ, int MODE>
+//
+// YB (planes of more than 512 threads' points): the plane is split over nyblk
+// CTAs of NYB rows; each CTA's ring holds its rows and 4 halo rows on each side.
+template <typename R, int RZ, int MODE, bool YB>
 __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
   using T = C2<R>;
   constexpr int NR = PassGeom<R>::NR;
@@ -156,13 +166,22 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
   const int NLy = a.NLy, NLz = a.NLz, NYZ = NLy * NLz;
   const bool with_w = a.W != nullptr;
   const bool do_export = a.S != nullptr;
+  const int nyblk = YB ? a.nyblk : 1;
+  const int RYZ = YB ? (a.NYB + 8) * NLz : NYZ;  // ring plane size
   T* ring = reinterpret_cast<T*>(smem_raw);
-  T* wring = ring + (size_t)NR * NYZ;  // [NR][maxpts] W chunks of the ring's planes
-  int* spo = reinterpret_cast<int*>(wring + (with_w ? (size_t)NR * a.maxpts : 0));  // sp_off[0..NLx]
-  for (int i = threadIdx.x; i <= a.NLx; i += blockDim.x) spo[i] = a.sp_off[i];
+  T* wring = ring + (size_t)NR * RYZ;  // [NR][maxpts] W chunks of the ring's planes
+  // sp_off[0..NLx] (or sp_blk in the YB form)
+  int* spo = reinterpret_cast<int*>(wring + (with_w ? (size_t)NR * a.maxpts : 0));
+  if constexpr (YB) {
+    for (int i = threadIdx.x; i < a.NLx * (nyblk + 1); i += blockDim.x) spo[i] = a.sp_blk[i];
+  } else {
+    for (int i = threadIdx.x; i <= a.NLx; i += blockDim.x) spo[i] = a.sp_off[i];
+  }
   __syncthreads();
 
-  const int b = blockIdx.x;
+  const int b = YB ? blockIdx.x / nyblk : blockIdx.x;
+  const int yb = YB ? blockIdx.x - b * nyblk : 0;
+  const int y0 = YB ? yb * a.NYB : 0;
   const int o = a.o_beg + b;
   const int kl = o / a.NBocc;
   const double kxd = a.kAc[3 * kl], kyd = a.kAc[3 * kl + 1], kzd = a.kAc[3 * kl + 2];
@@ -174,10 +193,13 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
   const int NZG = NLz / RZ;
   const int t = threadIdx.x;
   const int bd = blockDim.x;
-  const bool act = t < NLy * NZG;
-  const int y = act ? t / NZG : 0;
-  const int z0 = act ? (t - y * NZG) * RZ : 0;
-  const int own = y * NLz + z0;
+  const int ny_own = YB ? min(a.NYB, NLy - y0) : NLy;
+  const bool act = t < ny_own * NZG;
+  const int yl = act ? t / NZG : 0;  // row in the block
+  const int y = y0 + yl;             // row in the plane
+  const int z0 = act ? (t - yl * NZG) * RZ : 0;
+  const int own = y * NLz + z0;                       // in the plane
+  const int own_r = YB ? (4 + yl) * NLz + z0 : own;   // in the ring
 
   const int x_beg = blockIdx.y * a.SX;
   const int x_end = min(x_beg + a.SX, a.NLx);
@@ -192,9 +214,24 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
   auto refill = [&](int jn) {
     int p = x_beg + jn;
     while (p >= a.NLx) p -= a.NLx;
-    if (act && jn < nplanes) cp_run<R, RZ>(ring + (size_t)(jn % NR) * NYZ + own, inb + (size_t)p * NYZ + own);
+    if constexpr (YB) {
+      if (jn < nplanes) {  // the block's rows and the halo rows, periodic in y
+        T* dst = ring + (size_t)(jn % NR) * RYZ;
+        const T* src = inb + (size_t)p * NYZ;
+        for (int idx = t; idx < (a.NYB + 8) * NZG; idx += bd) {
+          const int r = idx / NZG, zz = (idx - r * NZG) * RZ;
+          int gy = y0 - 4 + r;
+          gy += gy < 0 ? NLy : 0;
+          gy -= gy >= NLy ? NLy : 0;
+          cp_run<R, RZ>(dst + r * NLz + zz, src + gy * NLz + zz);
+        }
+      }
+    } else {
+      if (act && jn < nplanes) cp_run<R, RZ>(ring + (size_t)(jn % NR) * NYZ + own, inb + (size_t)p * NYZ + own);
+    }
     if (with_w && jn < nown) {
-      const int q0 = spo[p], q1 = spo[p + 1];
+      const int q0 = YB ? spo[p * (nyblk + 1) + yb] : spo[p];
+      const int q1 = YB ? spo[p * (nyblk + 1) + yb + 1] : spo[p + 1];
       T* dst = wring + (size_t)(jn % NR) * a.maxpts;
       for (int qq = q0 + t; qq < q1; qq += bd) cp_run<R, 1>(dst + (qq - q0), Wb + qq);
     }
@@ -203,16 +240,16 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
 #pragma unroll 1
   for (int n = 0; n < NR - 1; ++n) refill(n);
 
-  int yo[8];
+  int yo[8];  // ring offsets of the y neighbours
 #pragma unroll
   for (int n = 1; n <= 4; ++n) {
-    yo[n - 1] = wrapi(y + n, NLy) * NLz + z0;
-    yo[3 + n] = wrapi(y - n, NLy) * NLz + z0;
+    yo[n - 1] = (YB ? 4 + yl + n : wrapi(y + n, NLy)) * NLz + z0;
+    yo[3 + n] = (YB ? 4 + yl - n : wrapi(y - n, NLy)) * NLz + z0;
   }
   constexpr int NZZ = RZ + 8;  // z runs start at z0-4, z0-4+RZ, ..., z0+4
   int zoff[NZZ / RZ];
 #pragma unroll
-  for (int m = 0; m < NZZ / RZ; ++m) zoff[m] = y * NLz + wrapi(z0 + m * RZ - 4, NLz);
+  for (int m = 0; m < NZZ / RZ; ++m) zoff[m] = (YB ? 4 + yl : y) * NLz + wrapi(z0 + m * RZ - 4, NLz);
 
   // register queue: in the march step of phase P (plane x = x_beg + 9i + P),
   // plane x-4+m sits in q[(P+m) % 9]; the march is unrolled nine times so the
@@ -239,16 +276,16 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
     cp_async_wait<NR - 6>();  // this thread's copies of planes <= x+4 have landed
     __syncthreads();          // ... and everyone's; the slot of plane x-1 is free
     refill(j + NR - 1);
-    const T* pl = ring + (size_t)(j % NR) * NYZ;
+    const T* pl = ring + (size_t)(j % NR) * RYZ;
     const bool more = x + 1 < x_end;
     if (act) {
       if constexpr (P == 0) {
         if (j == 0) {
 #pragma unroll
-          for (int n = 4; n < 8; ++n) lds_run<R, RZ>(q[n], ring + (size_t)(n - 4) * NYZ + own);
+          for (int n = 4; n < 8; ++n) lds_run<R, RZ>(q[n], ring + (size_t)(n - 4) * RYZ + own_r);
         }
       }
-      lds_run<R, RZ>(q[(P + 8) % 9], ring + (size_t)((j + 4) % NR) * NYZ + own);
+      lds_run<R, RZ>(q[(P + 8) % 9], ring + (size_t)((j + 4) % NR) * RYZ + own_r);
       const size_t pbase = (size_t)x * NYZ + own;
       R vln[RZ];
       int lqn[RZ];
@@ -324,7 +361,9 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
         w[r].y = fma(kx, wa[r].y, w[r].y);
       }
 
-      const T* wpl = wring + (size_t)(j % NR) * a.maxpts;
+      // plane-relative sphere index lq -> this block's W chunk
+      const T* wpl = wring + (size_t)(j % NR) * a.maxpts -
+                     (YB ? spo[x * (nyblk + 1) + yb] - spo[x * (nyblk + 1)] : 0);
       T res[RZ];
 #pragma unroll
       for (int r = 0; r < RZ; ++r) {
@@ -358,7 +397,7 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
         st_run<R, RZ>(a.out + (size_t)b * a.NL + pbase, res);
       }
       if (do_export) {  // the output at the sphere points, for the next projections
-        const int q0 = spo[x];
+        const int q0 = YB ? spo[x * (nyblk + 1)] : spo[x];
 #pragma unroll
         for (int r = 0; r < RZ; ++r)
           if (lq[r] >= 0) Sb[q0 + lq[r]] = res[r];
@@ -407,17 +446,20 @@ static cudaError_t launch_pass_t(const System& s, const PassIO& io, int o_beg, i
       a.nabc[4 * d + n] = (R)s.nab[d][n + 1];
     }
   a.sp_off = s.sp_off;
+  a.nyblk = s.nyblk;
+  a.NYB = s.nyblk > 1 ? s.NYB : s.NLy;
+  a.sp_blk = s.sp_blk;
   a.lqi = s.lqi;
   a.W = (const C2<R>*)io.W;
   a.S = (C2<R>*)io.S;
   a.nsp = s.nsp;
   a.maxpts = s.maxpts;
   for (int n = 0; n < 4; ++n) a.zf[n] = mk<R>((R)io.zfac[n][0], (R)io.zfac[n][1]);
-  const int nthr = s.NLy * (s.NLz / RZ);
+  const int nthr = a.NYB * (s.NLz / RZ);
   const int block = ((nthr + 31) / 32) * 32;
   const size_t smem = pass_smem_bytes(std::is_same<R, float>::value ? SGPU_PREC_C64 : SGPU_PREC_C128, s.NLy, s.NLz,
-                                      s.maxpts, io.W != nullptr, s.NLx);
-  auto kern = k_hpsi_pass<R, RZ, MODE>;
+                                      s.maxpts, io.W != nullptr, s.NLx, s.nyblk, a.NYB);
+  auto kern = s.nyblk > 1 ? k_hpsi_pass<R, RZ, MODE, true> : k_hpsi_pass<R, RZ, MODE, false>;
   if (smem > 48 * 1024) {
     // set outside stream capture (prepare_pass sets it before a capture)
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -428,7 +470,7 @@ static cudaError_t launch_pass_t(const System& s, const PassIO& io, int o_beg, i
       if (e != cudaSuccess) return e;
     }
   }
-  dim3 grid(nb, (s.NLx + a.SX - 1) / a.SX);
+  dim3 grid(nb * s.nyblk, (s.NLx + a.SX - 1) / a.SX);
   kern<<<grid, block, smem, s.launch_stream()>>>(a);
   return cudaGetLastError();
 }
@@ -454,13 +496,22 @@ cudaError_t launch_hpsi_pass(const System& s, int mode, const PassIO& io, int o_
 
 template <typename R, int RZ>
 static cudaError_t prepare_pass_rz(const System& s) {
-  const size_t smem =
-      pass_smem_bytes(std::is_same<R, float>::value ? SGPU_PREC_C64 : SGPU_PREC_C128, s.NLy, s.NLz, s.maxpts, true, s.NLx);
+  const size_t smem = pass_smem_bytes(std::is_same<R, float>::value ? SGPU_PREC_C64 : SGPU_PREC_C128, s.NLy, s.NLz,
+                                      s.maxpts, true, s.NLx, s.nyblk, s.nyblk > 1 ? s.NYB : s.NLy);
   if (smem <= 48 * 1024) return cudaSuccess;
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute(k_hpsi_pass<R, RZ, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
-  if ((e = cudaFuncSetAttribute(k_hpsi_pass<R, RZ, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
-  return cudaFuncSetAttribute(k_hpsi_pass<R, RZ, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (s.nyblk > 1) {
+    if ((e = cudaFuncSetAttribute(k_hpsi_pass<R, RZ, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+      return e;
+    if ((e = cudaFuncSetAttribute(k_hpsi_pass<R, RZ, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+      return e;
+    return cudaFuncSetAttribute(k_hpsi_pass<R, RZ, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  }
+  if ((e = cudaFuncSetAttribute(k_hpsi_pass<R, RZ, 0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+    return e;
+  if ((e = cudaFuncSetAttribute(k_hpsi_pass<R, RZ, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+    return e;
+  return cudaFuncSetAttribute(k_hpsi_pass<R, RZ, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
 cudaError_t prepare_pass(const System& s) {
@@ -470,7 +521,7 @@ cudaError_t prepare_pass(const System& s) {
   return rz2 ? prepare_pass_rz<double, 2>(s) : prepare_pass_rz<double, 1>(s);
 }
 
-int pass_block_threads(int NLy, int NLz) {
+int pass_block_threads(int NLy, int NLz) {  // without y-blocks
   const int rz = (NLz % 2) == 0 ? 2 : 1;
   return ((NLy * (NLz / rz) + 31) / 32) * 32;
 }

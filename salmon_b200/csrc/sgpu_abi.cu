@@ -151,8 +151,14 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
   if (d->Nlma > 0 && (!d->Mps || !d->Jxyz || !d->Jxx || !d->Jyy || !d->Jzz || !d->uV || !d->iuV || !d->a_tbl))
     return fail(SGPU_ERR_ARG, "sgpu_create: projector tables missing");
   const int rz = (d->NLz % 2 == 0) ? 2 : 1;
-  if ((long)d->NLy * (d->NLz / rz) > 512)
-    return fail(SGPU_ERR_UNSUPPORTED, "sgpu_create: NLy*NLz/" + std::to_string(rz) + " > 512 threads per plane");
+  // planes of more than 512 threads' points are split over y-blocks of >= 4 rows
+  const int nzg = d->NLz / rz;
+  if (nzg > 128) return fail(SGPU_ERR_UNSUPPORTED, "sgpu_create: NLz too large for the stencil pass");
+  int nyblk = 1, NYB = d->NLy;
+  if ((long)d->NLy * nzg > 512) {
+    nyblk = (d->NLy + 512 / nzg - 1) / (512 / nzg);
+    NYB = (d->NLy + nyblk - 1) / nyblk;
+  }
   const long NL = (long)d->NLx * d->NLy * d->NLz;
   if (NL > (1L << 30)) return fail(SGPU_ERR_ARG, "sgpu_create: grid too large");
 
@@ -168,6 +174,8 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
   if (e != cudaSuccess) { delete s; return cuda_fail(e, "cudaStreamCreate"); }
 
   s->prec = precision;
+  s->nyblk = nyblk;
+  s->NYB = NYB;
   s->NLx = d->NLx; s->NLy = d->NLy; s->NLz = d->NLz; s->NL = (int)NL;
   s->NK = d->NK; s->NK_s = d->NK_s; s->NK_e = d->NK_e; s->nkl = d->NK_e - d->NK_s + 1;
   s->NB = d->NB; s->NBocc = d->NBoccmax; s->norb = s->nkl * s->NBocc;
@@ -244,7 +252,7 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
   // packed projector points to sphere points
   std::vector<int> sp_off(s->NLx + 1, 0), q_of(s->NL, -1), qmap(std::max(1, s->NPI), 0);
   std::vector<int4> rec;
-  std::vector<int> cont, kbq, kb_multi;
+  std::vector<int> cont, kbq, kb_multi, qrow;
   {
     if (s->Nps >= 65536 || s->Nlma >= 32768)
       return bail(fail(SGPU_ERR_UNSUPPORTED, "sgpu_create: Nps must be < 65536 and Nlma < 32768"));
@@ -266,6 +274,7 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
         rec.push_back(make_int4(i - x * NYZ, std::min(c, 4), e[0], e[1]));
         rec.push_back(make_int4(e[2], e[3], c0, std::max(c - 4, 0)));
         q_of[i] = nsp++;
+        qrow.push_back(i / s->NLz);  // x*NLy + y
       }
     }
     sp_off[s->NLx] = nsp;
@@ -287,7 +296,7 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
   for (int i = 0; i < s->NL; ++i)
     if (q_of[i] >= 0) lqi[i] = (short)(q_of[i] - sp_off[i / (s->NLy * s->NLz)]);
   for (int pr = 0; pr < 2; ++pr)
-    if (sgpu::pass_smem_bytes(pr, s->NLy, s->NLz, s->maxpts, true, s->NLx) > 227 * 1024)
+    if (sgpu::pass_smem_bytes(pr, s->NLy, s->NLz, s->maxpts, true, s->NLx, s->nyblk, s->NYB) > 227 * 1024)
       return bail(fail(SGPU_ERR_UNSUPPORTED, "sgpu_create: an NLy x NLz plane ring does not fit in shared memory"));
   std::vector<double> uv((size_t)s->Nlma * s->Nps);
   if (s->Nlma) std::memcpy(uv.data(), d->uV, uv.size() * sizeof(double));
@@ -317,6 +326,20 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
   UP(s->kbq, kbq);
   UP(s->kb_multi, kb_multi);
   UP(s->lqi, lqi);
+  {  // sp_blk: first sphere point of every (plane, y-block) and the plane end
+    const int nb1 = s->nyblk + 1;
+    std::vector<int> cnt((size_t)s->NLx * s->nyblk, 0), blk((size_t)s->NLx * nb1, 0);
+    for (int r : qrow) cnt[(size_t)(r / s->NLy) * s->nyblk + (r % s->NLy) / s->NYB]++;
+    int acc = 0;
+    for (int x = 0; x < s->NLx; ++x) {
+      for (int yb = 0; yb < s->nyblk; ++yb) {
+        blk[(size_t)x * nb1 + yb] = acc;
+        acc += cnt[(size_t)x * s->nyblk + yb];
+      }
+      blk[(size_t)x * nb1 + s->nyblk] = acc;
+    }
+    UP(s->sp_blk, blk);
+  }
   UP(s->occ_o, occo);
 #undef UP
   const size_t nz = (size_t)s->nkl * s->Nlma * s->Nps;
@@ -367,7 +390,7 @@ int sgpu_destroy(sgpu_handle h) {
                   s->U, s->Uw, s->red, s->stage};
   for (void* p : bufs) cudaFree(p);
   void* gbufs[] = {s->gs_zu, s->gs_aux, s->gs_W, s->gs_st, s->gs_part, s->gs_A, s->gs_V, s->gs_w, s->gs_sweeps,
-                   s->occ_gs, s->gs_out, s->gs_res, s->gs_tb, s->vpsl, s->rho_d, s->exc_d};
+                   s->occ_gs, s->gs_out, s->gs_res, s->gs_tb, s->vpsl, s->rho_d, s->exc_d, s->sp_blk};
   for (void* p : gbufs) cudaFree(p);
   if (s->gs_h) cudaFreeHost(s->gs_h);
   if (s->red_h) cudaFreeHost(s->red_h);

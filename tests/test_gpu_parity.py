@@ -24,6 +24,9 @@ CASES = {
     "ragged_odd_z": lambda: S.small_system(9, 8, 11, nk=2, nb=3, seed=22),
     "microbench_20": lambda: S.microbench_system(20, nk_limit=2, Nb=32),
     "microbench_16": lambda: S.microbench_system(16, nk_limit=1, Nb=32),
+    # planes wider than one CTA (NLy*NLz/2 > 512): the pass splits them into y-blocks
+    "wide_48": lambda: S.microbench_system(48, nk_limit=1, Nb=4),
+    "wide_ragged": lambda: S.small_system(6, 50, 22, nk=2, nb=3, a=(5.0, 12.0, 9.0), seed=23),
 }
 
 
