@@ -57,6 +57,7 @@ def parse():
     p.add_argument("--no-precision", action="store_true", help="skip the FP32-vs-FP64 J(t) run")
     p.add_argument("--no-batched", action="store_true", help="skip the batched-systems run")
     p.add_argument("--batched-steps", type=int, default=1000)
+    p.add_argument("--no-large", action="store_true", help="skip the Si216 48^3 run")
     return p.parse_args()
 
 
@@ -267,6 +268,48 @@ def batched_bench(nsteps=1000, per_replay=10):
                         "synthetic Gaussian projectors / V_loc"}
 
 
+def large_bench(nsteps=10):
+    """The Si216 RT shape: 3x3x3 diamond supercell, 48^3 grid (planes split into
+    y-blocks), 2x2x1 = 4 k-points, 432 bands (1728 orbitals); seeded random
+    orbitals made on the device; Taylor-step throughput in complex(4) (launch
+    shapes autotuned) and complex(8)."""
+    import torch
+    from salmon_b200 import system as S
+    from salmon_b200.rt import GpuSystem
+    sysm, kAc, vloc, _ = S.si_supercell_system((3, 3, 3), (48, 48, 48), (2, 2, 1), 432, with_orbitals=False)
+    norb = sysm.nk_local * sysm.NBoccmax
+    gen = torch.Generator(device="cuda").manual_seed(S.SEED)
+    z = torch.randn((norb, sysm.NL), dtype=torch.complex128, device="cuda", generator=gen) / np.sqrt(sysm.NL * sysm.Hxyz)
+    out = {"workload": "Si216 48^3, 4 k x 432 bands (1728 orbitals), synthetic Gaussian projectors / V_loc"}
+    for prec in ("c64", "c128"):
+        g = GpuSystem(sysm, prec)
+        torch.cuda.synchronize()
+        g.set_state_dev(z.data_ptr())
+        g.set_vloc(vloc)
+        g.update_projector(kAc)
+        tuned = g.autotune(reps=2) if prec == "c64" else None
+        st = torch.cuda.ExternalStream(g.stream)
+        for _ in range(2):
+            g.hamiltonian(DT)
+        g.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(nsteps):
+            g.hamiltonian(DT)
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / nsteps
+        out[prec] = {"ms_per_step": ms, "orbital_updates_per_s": norb / (ms * 1e-3),
+                     "stencil_pass_ms": g.time_kernel("stencil_pass", reps=3)}
+        if tuned:
+            out[prec]["tuned"] = {"nslab": tuned[0], "uvpsi_split": tuned[1]}
+        g.close()
+    del z
+    out["fp32_over_fp64"] = out["c64"]["orbital_updates_per_s"] / out["c128"]["orbital_updates_per_s"]
+    return out
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -403,6 +446,9 @@ def main():
     batched = None
     if rank == 0 and not (args.only or args.no_e2e or args.no_batched):
         batched = batched_bench(args.batched_steps)
+    large = None
+    if rank == 0 and not (args.only or args.no_e2e or args.no_large):
+        large = large_bench()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -439,6 +485,7 @@ def main():
             "gpu_launches": h["launches"],
             "precision": prec_check,
             "batched": batched,
+            "large": large,
             "clocks": clocks,
         }
         print(json.dumps(out))

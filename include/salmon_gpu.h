@@ -126,6 +126,11 @@ void* sgpu_stream(sgpu_handle h);
  * RT/dt_evolve.f90:530). */
 int sgpu_set_state(sgpu_handle h, const double* zu /* complex(8), HOST */);
 
+/* The same from a DEV complex(8) array of the same layout, e.g. zu_t that an
+ * OpenACC host keeps on the device (`host_data use_device(zu_t)`); no host
+ * round trip. */
+int sgpu_set_state_dev(sgpu_handle h, const void* zu_dev);
+
 /* device -> HOST zu.  Replaces `update self(zu_t)` (control_sc.f90:215,395,414). */
 int sgpu_get_state(sgpu_handle h, double* zu /* complex(8), HOST */);
 

@@ -25,6 +25,7 @@ ABI = {
     "sgpu_stream": (C.c_void_p, [_vp]),
     "sgpu_set_state": (C.c_int, [_vp, _vp]),
     "sgpu_get_state": (C.c_int, [_vp, _vp]),
+    "sgpu_set_state_dev": (C.c_int, [_vp, _vp]),
     "sgpu_state_ptr": (C.c_void_p, [_vp]),
     "sgpu_set_vloc": (C.c_int, [_vp, _vp]),
     "sgpu_set_vpsl": (C.c_int, [_vp, _vp]),

@@ -428,6 +428,20 @@ int sgpu_set_state(sgpu_handle h, const double* zu) {
   return 0;
 }
 
+int sgpu_set_state_dev(sgpu_handle h, const void* zu_dev) {
+  if (!valid(h) || !zu_dev) return fail(SGPU_ERR_ARG, "sgpu_set_state_dev: null argument");
+  System* s = h;
+  const size_t n = (size_t)s->norb * s->NL;
+  if (s->prec == SGPU_PREC_C128)
+    CK(cudaMemcpyAsync(s->zu, zu_dev, n * sizeof(double2), cudaMemcpyDeviceToDevice, s->stream));
+  else
+    CK(sgpu::launch_c128_to_c64(static_cast<const double2*>(zu_dev), (float2*)s->zu, n, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  s->have_state = true;
+  s->S_valid = false;
+  return 0;
+}
+
 int sgpu_get_state(sgpu_handle h, double* zu) {
   if (!valid(h) || !zu) return fail(SGPU_ERR_ARG, "sgpu_get_state: null argument");
   System* s = h;

@@ -84,6 +84,10 @@ class GpuSystem:
             raise ValueError(f"zu must have shape {(s.nk_local, s.NBoccmax, s.NL)}, got {zu.shape}")
         call("sgpu_set_state", self._h, _vp(zu))
 
+    def set_state_dev(self, zu_dev: int):
+        """Resident orbitals from a device complex(8) array zu(NL,NBoccmax,NK_s:NK_e)."""
+        call("sgpu_set_state_dev", self._h, C.c_void_p(zu_dev))
+
     def get_state(self):
         s = self.sysm
         zu = np.empty((s.nk_local, s.NBoccmax, s.NL), np.complex128)

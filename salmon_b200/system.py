@@ -245,20 +245,26 @@ def calc_jxyz(NLx, NLy, NLz, aL, Rion, Rps):
     index order.  Returns Mps (NI,), Jxyz (1-based), Jxx, Jyy, Jzz as (NI, Nps)
     and the distance components (NI, Nps, 3) from the atom image."""
     h = np.asarray(aL) / np.array([NLx, NLy, NLz])
-    ix, iy, iz = np.meshgrid(np.arange(NLx), np.arange(NLy), np.arange(NLz), indexing="ij")
-    mx, my, mz = ix.ravel(), iy.ravel(), iz.ravel()
+    N = (NLx, NLy, NLz)
     per_atom = []
     for a in range(Rion.shape[0]):
         js, jx, jy, jz, dv = [], [], [], [], []
         for ax in range(-2, 3):
             for ay in range(-2, 3):
                 for az in range(-2, 3):
-                    tx = Rion[a, 0] + ax * aL[0]
-                    ty = Rion[a, 1] + ay * aL[1]
-                    tz = Rion[a, 2] + az * aL[2]
-                    x = mx * h[0] - tx
-                    y = my * h[1] - ty
-                    z = mz * h[2] - tz
+                    t = Rion[a] + np.array([ax, ay, az]) * np.asarray(aL)
+                    # only the grid box around the image can be inside the sphere; the box
+                    # is enumerated in grid-index order, like the full grid
+                    lo = [max(0, int(np.floor((t[d] - Rps) / h[d]))) for d in range(3)]
+                    hi = [min(N[d] - 1, int(np.ceil((t[d] + Rps) / h[d]))) for d in range(3)]
+                    if any(lo[d] > hi[d] for d in range(3)):
+                        continue
+                    bx, by, bz = np.meshgrid(np.arange(lo[0], hi[0] + 1), np.arange(lo[1], hi[1] + 1),
+                                             np.arange(lo[2], hi[2] + 1), indexing="ij")
+                    mx, my, mz = bx.ravel(), by.ravel(), bz.ravel()
+                    x = mx * h[0] - t[0]
+                    y = my * h[1] - t[1]
+                    z = mz * h[2] - t[2]
                     r = np.sqrt(x * x + y * y + z * z)
                     sel = np.nonzero(r < Rps)[0]
                     if sel.size:
@@ -304,20 +310,42 @@ def gaussian_projectors(Mps, dist, Hxyz, rc=2.0):
     return uV, iuV, a_tbl
 
 
-def periodic_gaussian_vloc(NLx, NLy, NLz, aL, centres, depth, width):
-    """V(r) = -sum_a D_a exp(-|r-R_a|^2/w_a^2) summed over the 27 nearest images."""
+def periodic_gaussian_vloc(NLx, NLy, NLz, aL, centres, depth, width, cutoff=None):
+    """V(r) = -sum_a D_a exp(-|r-R_a|^2/w_a^2) summed over the 27 nearest images.
+    With `cutoff` (in widths), an image only adds to the grid box within
+    cutoff*w of it (a large cell's potential in seconds instead of minutes; the
+    dropped terms are below exp(-cutoff^2) of the depth)."""
     h = np.asarray(aL) / np.array([NLx, NLy, NLz])
-    ix, iy, iz = np.meshgrid(np.arange(NLx), np.arange(NLy), np.arange(NLz), indexing="ij")
-    r = np.stack([ix.ravel() * h[0], iy.ravel() * h[1], iz.ravel() * h[2]], axis=1)
-    v = np.zeros(r.shape[0])
+    N = (NLx, NLy, NLz)
+    if cutoff is None:
+        ix, iy, iz = np.meshgrid(np.arange(NLx), np.arange(NLy), np.arange(NLz), indexing="ij")
+        r = np.stack([ix.ravel() * h[0], iy.ravel() * h[1], iz.ravel() * h[2]], axis=1)
+        v = np.zeros(r.shape[0])
+        for a in range(centres.shape[0]):
+            for ax in (-1, 0, 1):
+                for ay in (-1, 0, 1):
+                    for az in (-1, 0, 1):
+                        c = centres[a] + np.array([ax, ay, az]) * aL
+                        d2 = ((r - c) ** 2).sum(axis=1)
+                        v -= depth[a] * np.exp(-d2 / width[a] ** 2)
+        return v
+    v = np.zeros((NLx, NLy, NLz))
     for a in range(centres.shape[0]):
+        rc = cutoff * width[a]
         for ax in (-1, 0, 1):
             for ay in (-1, 0, 1):
                 for az in (-1, 0, 1):
                     c = centres[a] + np.array([ax, ay, az]) * aL
-                    d2 = ((r - c) ** 2).sum(axis=1)
-                    v -= depth[a] * np.exp(-d2 / width[a] ** 2)
-    return v
+                    lo = [max(0, int(np.floor((c[d] - rc) / h[d]))) for d in range(3)]
+                    hi = [min(N[d] - 1, int(np.ceil((c[d] + rc) / h[d]))) for d in range(3)]
+                    if any(lo[d] > hi[d] for d in range(3)):
+                        continue
+                    gx = np.arange(lo[0], hi[0] + 1) * h[0] - c[0]
+                    gy = np.arange(lo[1], hi[1] + 1) * h[1] - c[1]
+                    gz = np.arange(lo[2], hi[2] + 1) * h[2] - c[2]
+                    d2 = gx[:, None, None] ** 2 + gy[None, :, None] ** 2 + gz[None, None, :] ** 2
+                    v[lo[0]:hi[0] + 1, lo[1]:hi[1] + 1, lo[2]:hi[2] + 1] -= depth[a] * np.exp(-d2 / width[a] ** 2)
+    return v.ravel()
 
 
 def orthonormalise(zu, Hxyz):
@@ -398,7 +426,8 @@ def si_supercell_system(ncell=(1, 1, 1), grid=(16, 16, 16), nkgrid=(4, 4, 4), Nb
     uV, iuV, a_tbl = gaussian_projectors(Mps, dist, Hxyz)
     depth = rng.uniform(0.5, 2.0, Rion.shape[0])
     width = rng.uniform(1.0, 2.0, Rion.shape[0])
-    vloc = periodic_gaussian_vloc(NLx, NLy, NLz, aL, Rion, depth, width)
+    # large supercells: images only near the grid box they reach (see periodic_gaussian_vloc)
+    vloc = periodic_gaussian_vloc(NLx, NLy, NLz, aL, Rion, depth, width, cutoff=8.0 if Rion.shape[0] > 64 else None)
     sysm = System(NLx=NLx, NLy=NLy, NLz=NLz, aL=aL, kAc0=kAc0, NB=Nb, NBoccmax=Nocc, occ=occ, Rion=Rion, Rps=2.0,
                   Mps=Mps, Jxyz=Jxyz, Jxx=Jxx, Jyy=Jyy, Jzz=Jzz, uV=uV, iuV=iuV, a_tbl=a_tbl)
     sysm.extra.update(seed=seed, depth=depth, width=width)
