@@ -58,6 +58,7 @@ def parse():
     p.add_argument("--no-batched", action="store_true", help="skip the batched-systems run")
     p.add_argument("--batched-steps", type=int, default=1000)
     p.add_argument("--no-large", action="store_true", help="skip the Si216 48^3 run")
+    p.add_argument("--precond", action="store_true", help="also run the Si64 CG preconditioner comparison (minutes)")
     return p.parse_args()
 
 
@@ -310,6 +311,57 @@ def large_bench(nsteps=10):
     return out
 
 
+def precond_bench(max_outer=60):
+    """CG to a 1e-8 residual on the Si64 ground-state shape (2x2x2 diamond
+    supercell, 32^3 grid, 2x2x2 k-points, 128 occupied + 16 empty bands, fixed
+    V_loc, FP64): the learned preconditioner, trained on residual/correction
+    pairs from plain CG on one displaced configuration (sigma = 0.05 bohr),
+    evaluated on another, against TPA alone and plain CG (capped at
+    `max_outer` iterations)."""
+    from oracle import net_oracle as N   # the identity weights the network starts from
+    from salmon_b200 import precond as P
+    from salmon_b200.rt import GpuSystem
+    base = dict(ncell=(2, 2, 2), grid=(32, 32, 32), nkgrid=(2, 2, 2), Nb=144, Nocc=128)
+
+    def gpu(seed):
+        sysm, kAc, vloc, zu = P.displaced_system(base, 0.05, seed=seed)
+        g = GpuSystem(sysm, "c128")
+        g.set_vloc(vloc)
+        g.update_projector(kAc)
+        g.gs_set_state(zu)
+        g.set_cg_delta(1e-24)
+        return sysm, g
+
+    t0 = time.perf_counter()
+    sysm, g = gpu(101)
+    R, E, kidx, tb = P.cg_training_pairs(g, sysm, 128, snap_at=(10, 20, 40), bands=(0, 31, 63, 95, 127))
+    g.net_set_weights(N.identity_weights(noise=1e-2, seed=0))
+    hist = P.train(g, P.tpa_inputs(g, R, kidx, tb), E, steps=400, batch=16, lr=2e-3)
+    w = g.net_get_weights()
+    g.close()
+    t_train = time.perf_counter() - t0
+    runs = {}
+    for kind in ("learned", "tpa", "plain"):
+        sysm, g = gpu(202)
+        if kind == "learned":
+            g.net_set_weights(w)
+        g.set_cg_preconditioner(kind)
+        t1 = time.perf_counter()
+        r = P.solve_to(g, tol=1e-8, ncg=4, max_outer=max_outer, nconv=128)
+        runs[kind] = {"outer": r["outer"], "cg_iterations": r["cg_iterations"], "residual": r["residual"],
+                      "converged": r["converged"], "seconds": time.perf_counter() - t1, "esp": r["esp"][:, :128]}
+        g.close()
+    de = float(np.abs(runs["learned"]["esp"] - runs["tpa"]["esp"]).max())
+    for r in runs.values():
+        r.pop("esp")
+    return {"runs": runs, "learned_vs_plain_iterations": runs["learned"]["cg_iterations"] / runs["plain"]["cg_iterations"],
+            "learned_vs_tpa_iterations": runs["learned"]["cg_iterations"] / runs["tpa"]["cg_iterations"],
+            "eigenvalue_max_abs_diff_learned_vs_tpa": de, "training_pairs": int(R.shape[0]),
+            "training_loss": [float(np.mean(hist[:5])), float(np.mean(hist[-20:]))], "training_seconds": t_train,
+            "workload": "Si64 32^3, 8 k x (128+16) bands, fixed V_loc, CG to residual 1e-8 (plain capped at "
+                        f"{max_outer} outer iterations)"}
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -449,6 +501,7 @@ def main():
     large = None
     if rank == 0 and not (args.only or args.no_e2e or args.no_large):
         large = large_bench()
+    pc = precond_bench() if (rank == 0 and args.precond) else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -486,6 +539,7 @@ def main():
             "precision": prec_check,
             "batched": batched,
             "large": large,
+            "precond": pc,
             "clocks": clocks,
         }
         print(json.dumps(out))

@@ -76,7 +76,7 @@ def _shifted_solve(g, ik, r, shift, iters, tol=1e-10):
     return t
 
 
-def correction_pairs(g, sysm, snaps, nconv, emin, margin=1.0, iters=80):
+def correction_pairs(g, sysm, snaps, nconv, emin, margin=1.0, iters=80, bands=None):
     """Residual/correction pairs from snapshots of plain CG.  For each of the
     lowest nconv bands psi of every snapshot: the gradient
     r = H psi - <psi|H|psi> psi, and the correction t that solves the shifted
@@ -89,13 +89,14 @@ def correction_pairs(g, sysm, snaps, nconv, emin, margin=1.0, iters=80):
     target flat over the occupied spectrum, as TPA is; a small margin
     over-weights the lowest states and a large one flattens the high-energy
     fall-off (both measured to slow CG down).  Returns complex arrays (n, NL) of r and t, and per pair the
-    local k-point index and the band's kinetic energy <psi|T|psi> (for TPA)."""
+    local k-point index and the band's kinetic energy <psi|T|psi> (for TPA).
+    `bands` restricts the pairs to those bands (default: all nconv)."""
     Hxyz = sysm.Hxyz
     R, E, K, TB = [], [], [], []
     for Z in snaps:
         for kl in range(sysm.nk_local):
             ik = sysm.NK_s + kl
-            for b in range(nconv):
+            for b in (range(nconv) if bands is None else bands):
                 psi = Z[kl, b]
                 hpsi, tpsi = g.hpsi_omp_KB_GS(ik, psi)
                 eps = float(np.vdot(psi, hpsi).real * Hxyz)
@@ -110,7 +111,7 @@ def correction_pairs(g, sysm, snaps, nconv, emin, margin=1.0, iters=80):
     return np.array(R), np.array(E), np.array(K, np.int32), np.array(TB)
 
 
-def cg_training_pairs(g, sysm, nconv, snap_at=(10, 20, 40, 60, 80), ncg=4, margin=1.0):
+def cg_training_pairs(g, sysm, nconv, snap_at=(10, 20, 40, 60, 80), ncg=4, margin=1.0, bands=None):
     """Runs the reference's plain CG from the loaded ground-state orbitals and
     keeps snapshots of the bands at the iterations in snap_at; the lowest
     eigenvalue of each k-point (for the shift) comes from converging further
@@ -125,7 +126,7 @@ def cg_training_pairs(g, sysm, nconv, snap_at=(10, 20, 40, 60, 80), ncg=4, margi
     g.set_cg_preconditioner("tpa")
     emin = solve_to(g, tol=1e-6, ncg=ncg, max_outer=200, nconv=1)["esp"][:, 0]
     g.set_cg_preconditioner("plain")
-    return correction_pairs(g, sysm, snaps, nconv, emin, margin=margin)
+    return correction_pairs(g, sysm, snaps, nconv, emin, margin=margin, bands=bands)
 
 
 def tpa_inputs(g, R, kidx, tband):
