@@ -36,7 +36,7 @@ sys.path.insert(0, ROOT)
 METRIC = "RT orbital-updates/s: FP32+FP64-reduce vs FP64 GPU at ΔJ<1e-5; hpsi %HBM peak"
 DT = 0.08
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one stencil-pass launch, per
-# orbital, from the capture in profiles/k_hpsi_pass_uvpsi_kbfield_c64_32cubed_864orb.md
+# orbital, from the capture in profiles/k_hpsi_pass_k_kb_fused_c64_32cubed_864orb.md
 # (864 orbitals; traffic grows with the orbital count).
 NCU_TRAFFIC_BYTES_PER_ORBITAL = {("stencil_pass", "c64", 32): 536.171264e6 / 864}
 
