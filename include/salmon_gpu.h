@@ -275,7 +275,10 @@ enum {
   SGPU_PARAM_NSLAB = 0,       /* CTAs per orbital along x in the stencil pass (1..NLx)              */
   SGPU_PARAM_LAUNCHES = 1,    /* kernels the handle has launched, modulo 2^31 (read; set 0 to reset) */
   SGPU_PARAM_UVPSI_SPLIT = 2, /* warps splitting the points of one projection tile: 1, 2, 4 or 8     */
-  SGPU_PARAM_CG_PRECOND = 3   /* sgpu_cg direction: SGPU_CG_PLAIN, SGPU_CG_TPA or SGPU_CG_LEARNED     */
+  SGPU_PARAM_CG_PRECOND = 3,  /* sgpu_cg direction: SGPU_CG_PLAIN, SGPU_CG_TPA or SGPU_CG_LEARNED     */
+  SGPU_PARAM_PASS_TABLES = 4  /* stencil pass: 1 stages Vloc and the sphere-index table of each plane
+                                 through shared memory with the plane (where it fits), 0 loads them
+                                 from global memory one plane ahead                                   */
 };
 
 /* CG preconditioners.  PLAIN is the reference's CG_ompk.  TPA multiplies the

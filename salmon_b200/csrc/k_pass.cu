@@ -43,6 +43,7 @@ struct PassArgs {
   double lap0sum;        // lapx(0)+lapy(0)+lapz(0)
   R lapt[12];            // lapx(1:4), lapy(1:4), lapz(1:4)
   R nabc[12];            // nabx(1:4), naby(1:4), nabz(1:4)
+  float2 cl2[12], cn2[12];  // complex(4): lapt and nabc as broadcast pairs for the packed FP32 arithmetic
   // Kleinman-Bylander term by plane: plane x's sphere points are
   // sp_off[x] .. sp_off[x+1]-1 (at most maxpts); lqi[i] is the index of grid
   // point i among its plane's sphere points, or -1.
@@ -67,6 +68,10 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
@@ -141,15 +146,42 @@ __device__ __forceinline__ void ld_lq(int (&d)[RZ], const short* p) {
 
 __device__ __forceinline__ int wrapi(int a, int n) { a %= n; return a < 0 ? a + n : a; }
 
+// v += cl (p + m), wa += cn (p - m).  Complex(4) runs on packed FP32 pairs
+// (sm_100 f32x2 add/fma: one instruction updates both parts of a complex
+// value; cl, cn are broadcast pairs); complex(8) on scalar FP64.
+__device__ __forceinline__ void stencil_pair(float2& v, float2& wa, float2 p, float2 m, float2 cl, float2 cn) {
+  const float2 sum = __fadd2_rn(p, m);
+  const float2 dif = __ffma2_rn(m, make_float2(-1.f, -1.f), p);  // p - m (exact negation)
+  v = __ffma2_rn(cl, sum, v);
+  wa = __ffma2_rn(cn, dif, wa);
+}
+__device__ __forceinline__ void stencil_pair(double2& v, double2& wa, double2 p, double2 m, double cl, double cn) {
+  v.x = fma(cl, p.x + m.x, v.x);
+  v.y = fma(cl, p.y + m.y, v.y);
+  wa.x = fma(cn, p.x - m.x, wa.x);
+  wa.y = fma(cn, p.y - m.y, wa.y);
+}
+template <typename R> __device__ __forceinline__ auto kpair(double k) {
+  if constexpr (std::is_same<R, float>::value) return make_float2((float)k, (float)k); else return k;
+}
+// w = k wa (first axis) or w += k wa
+__device__ __forceinline__ float2 kscale(float2 k, float2 wa, float2 w) { return __ffma2_rn(k, wa, w); }
+__device__ __forceinline__ double2 kscale(double k, double2 wa, double2 w) {
+  return make_double2(fma(k, wa.x, w.x), fma(k, wa.y, w.y));
+}
+
 template <typename R> struct PassGeom {
   static constexpr int NR = std::is_same<R, float>::value ? 8 : 6;  // ring planes
 };
 
-size_t pass_smem_bytes(int prec, int NLy, int NLz, int maxpts, bool with_w, int NLx, int nyblk, int NYB) {
+size_t pass_smem_bytes(int prec, int NLy, int NLz, int maxpts, bool with_w, int NLx, int nyblk, int NYB,
+                       bool tables) {
   const size_t e = prec == SGPU_PREC_C64 ? sizeof(float2) : sizeof(double2);
   const int NR = prec == SGPU_PREC_C64 ? PassGeom<float>::NR : PassGeom<double>::NR;
   const size_t ryz = nyblk > 1 ? (size_t)(NYB + 8) * NLz : (size_t)NLy * NLz;
-  return e * (size_t)NR * (ryz + (with_w ? (size_t)maxpts : 0)) + sizeof(int) * (size_t)NLx * (nyblk + 1) +
+  const size_t tyz = nyblk > 1 ? (size_t)NYB * NLz : (size_t)NLy * NLz;
+  return e * (size_t)NR * (ryz + (with_w ? (size_t)maxpts : 0)) +
+         (tables ? (size_t)NR * tyz * (e / 2 + sizeof(short)) : 0) + sizeof(int) * (size_t)NLx * (nyblk + 1) +
          sizeof(int);
 }
 
@@ -158,8 +190,13 @@ size_t pass_smem_bytes(int prec, int NLy, int NLz, int maxpts, bool with_w, int 
 //
 // YB (planes of more than 512 threads' points): the plane is split over nyblk
 // CTAs of NYB rows; each CTA's ring holds its rows and 4 halo rows on each side.
-template <typename R, int RZ, int MODE, bool YB>
+// TB (two-point form): Vloc and the local sphere indices of each owned plane
+// travel with the plane through the ring (copy group of the plane) instead of
+// being loaded from global memory one plane ahead; this takes the dependent
+// global loads off each march step.
+template <typename R, int RZ, int MODE, bool YB, bool TB>
 __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
+  static_assert(!TB || RZ == 2, "table staging copies the two points' entries as one run");
   using T = C2<R>;
   constexpr int NR = PassGeom<R>::NR;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -170,8 +207,12 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
   const int RYZ = YB ? (a.NYB + 8) * NLz : NYZ;  // ring plane size
   T* ring = reinterpret_cast<T*>(smem_raw);
   T* wring = ring + (size_t)NR * RYZ;  // [NR][maxpts] W chunks of the ring's planes
+  constexpr bool tab = TB;
+  const int TYZ = YB ? a.NYB * NLz : NYZ;  // table plane size (owned rows)
+  R* vtab = reinterpret_cast<R*>(wring + (with_w ? (size_t)NR * a.maxpts : 0));  // [NR][TYZ] (tab)
+  short* lqtab = reinterpret_cast<short*>(vtab + (tab ? (size_t)NR * TYZ : 0));    // [NR][TYZ] (tab)
   // sp_off[0..NLx] (or sp_blk in the YB form)
-  int* spo = reinterpret_cast<int*>(wring + (with_w ? (size_t)NR * a.maxpts : 0));
+  int* spo = reinterpret_cast<int*>(lqtab + (tab ? (size_t)NR * TYZ : 0));
   if constexpr (YB) {
     for (int i = threadIdx.x; i < a.NLx * (nyblk + 1); i += blockDim.x) spo[i] = a.sp_blk[i];
   } else {
@@ -188,7 +229,15 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
   const R A = (R)((kxd * kxd + kyd * kyd + kzd * kzd - a.lap0sum) * 0.5);  // k2lap0_2 (hpsi.f90:120-121)
   // nabt = k_d nab_d (hpsi.f90:122-124), applied once per axis:
   // w = sum_d k_d sum_n nab_d,n (psi(+n) - psi(-n))
-  const R kx = (R)kxd, ky = (R)kyd, kz = (R)kzd;
+  using KT = typename std::conditional<std::is_same<R, float>::value, float2, double>::type;
+  const KT kx = kpair<R>(kxd), ky = kpair<R>(kyd), kz = kpair<R>(kzd);
+  // FD coefficients: broadcast pairs for complex(4), scalars for complex(8)
+  auto CL = [&](int i) -> KT {
+    if constexpr (std::is_same<R, float>::value) return a.cl2[i]; else return a.lapt[i];
+  };
+  auto CN = [&](int i) -> KT {
+    if constexpr (std::is_same<R, float>::value) return a.cn2[i]; else return a.nabc[i];
+  };
 
   const int NZG = NLz / RZ;
   const int t = threadIdx.x;
@@ -200,6 +249,7 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
   const int z0 = act ? (t - yl * NZG) * RZ : 0;
   const int own = y * NLz + z0;                       // in the plane
   const int own_r = YB ? (4 + yl) * NLz + z0 : own;   // in the ring
+  const int own_t = YB ? yl * NLz + z0 : own;         // in the table planes
 
   const int x_beg = blockIdx.y * a.SX;
   const int x_end = min(x_beg + a.SX, a.NLx);
@@ -228,6 +278,14 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
       }
     } else {
       if (act && jn < nplanes) cp_run<R, RZ>(ring + (size_t)(jn % NR) * NYZ + own, inb + (size_t)p * NYZ + own);
+    }
+    if constexpr (TB) {
+      if (act && jn < nown) {
+        const size_t g = (size_t)p * NYZ + own;
+        R* vd = vtab + (size_t)(jn % NR) * TYZ + own_t;
+        if constexpr (sizeof(R) == 4) cp_async8(vd, a.vloc + g); else cp_async16(vd, a.vloc + g);
+        if (with_w || do_export) cp_async4(lqtab + (size_t)(jn % NR) * TYZ + own_t, a.lqi + g);
+      }
     }
     if (with_w && jn < nown) {
       const int q0 = YB ? spo[p * (nyblk + 1) + yb] : spo[p];
@@ -263,7 +321,7 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
   int lq[RZ];  // local sphere indices of the current plane, loaded one plane ahead
 #pragma unroll
   for (int r = 0; r < RZ; ++r) { vl[r] = (R)0; lq[r] = -1; }
-  if (act) {
+  if (act && !TB) {
 #pragma unroll
     for (int r = 0; r < RZ; ++r) vl[r] = __ldg(a.vloc + (size_t)x_beg * NYZ + own + r);
     if (with_w || do_export) ld_lq<RZ>(lq, a.lqi + (size_t)x_beg * NYZ + own);
@@ -291,7 +349,16 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
       int lqn[RZ];
 #pragma unroll
       for (int r = 0; r < RZ; ++r) { vln[r] = (R)0; lqn[r] = -1; }
-      if (more) {
+      if constexpr (TB) {  // this plane's tables arrived with it (copy group j)
+        const R* vs = vtab + (size_t)(j % NR) * TYZ + own_t;
+#pragma unroll
+        for (int r = 0; r < RZ; ++r) vl[r] = vs[r];
+        if (with_w || do_export) {
+          const int v2 = *reinterpret_cast<const int*>(lqtab + (size_t)(j % NR) * TYZ + own_t);
+          lq[0] = (int)(short)(v2 & 0xffff);
+          lq[RZ - 1] = v2 >> 16;
+        }
+      } else if (more) {
 #pragma unroll
         for (int r = 0; r < RZ; ++r) vln[r] = __ldg(a.vloc + pbase + NYZ + r);
         if (with_w || do_export) ld_lq<RZ>(lqn, a.lqi + pbase + NYZ);
@@ -299,67 +366,71 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
       T v[RZ], w[RZ], wa[RZ];
 #pragma unroll
       for (int r = 0; r < RZ; ++r) { v[r] = mk<R>(0, 0); wa[r] = mk<R>(0, 0); }
+      if constexpr (std::is_same<R, float>::value) {
+        // z: the values z0-4 .. z0+RZ+3 of plane x (the centre run from the queue), as pairs
+        T zv[NZZ];
 #pragma unroll
-      for (int m = 0; m < NZZ / RZ; ++m) {  // z: each value feeds every point it neighbours
-        T run[RZ];
-        if (m * RZ == 4) {
+        for (int m = 0; m < NZZ / RZ; ++m) {
+          T run[RZ];
+          if (m * RZ == 4) {
 #pragma unroll
-          for (int s2 = 0; s2 < RZ; ++s2) run[s2] = q[(P + 4) % 9][s2];
-        } else {
-          lds_run<R, RZ>(run, pl + zoff[m]);
+            for (int s2 = 0; s2 < RZ; ++s2) run[s2] = q[(P + 4) % 9][s2];
+          } else {
+            lds_run<R, RZ>(run, pl + zoff[m]);
+          }
+#pragma unroll
+          for (int s2 = 0; s2 < RZ; ++s2) zv[m * RZ + s2] = run[s2];
         }
 #pragma unroll
-        for (int s2 = 0; s2 < RZ; ++s2)
+        for (int n = 1; n <= 4; ++n)
 #pragma unroll
-          for (int r = 0; r < RZ; ++r) {
-            const int k = m * RZ + s2 - 4 - r;
-            if (k != 0 && k >= -4 && k <= 4) {
-              const int n = k > 0 ? k : -k;
-              const R cl = a.lapt[7 + n];
-              const R cn = k > 0 ? a.nabc[7 + n] : -a.nabc[7 + n];
-              v[r].x = fma(cl, run[s2].x, v[r].x);
-              v[r].y = fma(cl, run[s2].y, v[r].y);
-              wa[r].x = fma(cn, run[s2].x, wa[r].x);
-              wa[r].y = fma(cn, run[s2].y, wa[r].y);
-            }
+          for (int r = 0; r < RZ; ++r) stencil_pair(v[r], wa[r], zv[4 + r + n], zv[4 + r - n], CL(8 + n - 1), CN(8 + n - 1));
+      } else {
+#pragma unroll
+        for (int m = 0; m < NZZ / RZ; ++m) {  // z: each value feeds every point it neighbours, as it arrives
+          T run[RZ];
+          if (m * RZ == 4) {
+#pragma unroll
+            for (int s2 = 0; s2 < RZ; ++s2) run[s2] = q[(P + 4) % 9][s2];
+          } else {
+            lds_run<R, RZ>(run, pl + zoff[m]);
           }
+#pragma unroll
+          for (int s2 = 0; s2 < RZ; ++s2)
+#pragma unroll
+            for (int r = 0; r < RZ; ++r) {
+              const int k = m * RZ + s2 - 4 - r;
+              if (k != 0 && k >= -4 && k <= 4) {
+                const int n = k > 0 ? k : -k;
+                const R cl = a.lapt[7 + n];
+                const R cn = k > 0 ? a.nabc[7 + n] : -a.nabc[7 + n];
+                v[r].x = fma(cl, run[s2].x, v[r].x);
+                v[r].y = fma(cl, run[s2].y, v[r].y);
+                wa[r].x = fma(cn, run[s2].x, wa[r].x);
+                wa[r].y = fma(cn, run[s2].y, wa[r].y);
+              }
+            }
+        }
       }
 #pragma unroll
-      for (int r = 0; r < RZ; ++r) { w[r] = mk<R>(kz * wa[r].x, kz * wa[r].y); wa[r] = mk<R>(0, 0); }
+      for (int r = 0; r < RZ; ++r) { w[r] = kscale(kz, wa[r], mk<R>(0, 0)); wa[r] = mk<R>(0, 0); }
 #pragma unroll
       for (int n = 1; n <= 4; ++n) {  // y
         T rp[RZ], rm[RZ];
         lds_run<R, RZ>(rp, pl + yo[n - 1]);
         lds_run<R, RZ>(rm, pl + yo[3 + n]);
 #pragma unroll
-        for (int r = 0; r < RZ; ++r) {
-          v[r].x = fma(a.lapt[3 + n], rp[r].x + rm[r].x, v[r].x);
-          v[r].y = fma(a.lapt[3 + n], rp[r].y + rm[r].y, v[r].y);
-          wa[r].x = fma(a.nabc[3 + n], rp[r].x - rm[r].x, wa[r].x);
-          wa[r].y = fma(a.nabc[3 + n], rp[r].y - rm[r].y, wa[r].y);
-        }
+        for (int r = 0; r < RZ; ++r) stencil_pair(v[r], wa[r], rp[r], rm[r], CL(4 + n - 1), CN(4 + n - 1));
       }
 #pragma unroll
-      for (int r = 0; r < RZ; ++r) {
-        w[r].x = fma(ky, wa[r].x, w[r].x);
-        w[r].y = fma(ky, wa[r].y, w[r].y);
-        wa[r] = mk<R>(0, 0);
-      }
+      for (int r = 0; r < RZ; ++r) { w[r] = kscale(ky, wa[r], w[r]); wa[r] = mk<R>(0, 0); }
 #pragma unroll
       for (int n = 1; n <= 4; ++n)  // x: the register queue
 #pragma unroll
-        for (int r = 0; r < RZ; ++r) {
-          const T pp = q[(P + 4 + n) % 9][r], mm = q[(P + 4 - n) % 9][r];
-          v[r].x = fma(a.lapt[n - 1], pp.x + mm.x, v[r].x);
-          v[r].y = fma(a.lapt[n - 1], pp.y + mm.y, v[r].y);
-          wa[r].x = fma(a.nabc[n - 1], pp.x - mm.x, wa[r].x);
-          wa[r].y = fma(a.nabc[n - 1], pp.y - mm.y, wa[r].y);
-        }
+        for (int r = 0; r < RZ; ++r)
+          stencil_pair(v[r], wa[r], q[(P + 4 + n) % 9][r], q[(P + 4 - n) % 9][r], CL(n - 1), CN(n - 1));
 #pragma unroll
-      for (int r = 0; r < RZ; ++r) {
-        w[r].x = fma(kx, wa[r].x, w[r].x);
-        w[r].y = fma(kx, wa[r].y, w[r].y);
-      }
+      for (int r = 0; r < RZ; ++r) w[r] = kscale(kx, wa[r], w[r]);
 
       // plane-relative sphere index lq -> this block's W chunk
       const T* wpl = wring + (size_t)(j % NR) * a.maxpts -
@@ -402,8 +473,10 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
         for (int r = 0; r < RZ; ++r)
           if (lq[r] >= 0) Sb[q0 + lq[r]] = res[r];
       }
+      if constexpr (!TB) {
 #pragma unroll
-      for (int r = 0; r < RZ; ++r) { vl[r] = vln[r]; lq[r] = lqn[r]; }
+        for (int r = 0; r < RZ; ++r) { vl[r] = vln[r]; lq[r] = lqn[r]; }
+      }
     }
     ++x;
     return x < x_end;
@@ -423,6 +496,24 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
 }
 
 // ------------------------------------------------------------- launch ---
+// Vloc and sphere-index tables through the ring: two-point form, when both
+// precisions' rings still fit in shared memory with them
+static bool pass_tables(const System& s, int RZ) {
+  if (RZ != 2 || !s.pass_tab) return false;
+  const int NYB = s.nyblk > 1 ? s.NYB : s.NLy;
+  for (int pr = 0; pr < 2; ++pr)
+    if (pass_smem_bytes(pr, s.NLy, s.NLz, s.maxpts, true, s.NLx, s.nyblk, NYB, true) > 227 * 1024) return false;
+  return true;
+}
+
+template <typename R, int RZ, int MODE>
+static void (*pass_kernel(bool yb, bool tb))(const PassArgs<R>) {
+  if constexpr (RZ == 2) {
+    if (tb) return yb ? k_hpsi_pass<R, RZ, MODE, true, true> : k_hpsi_pass<R, RZ, MODE, false, true>;
+  }
+  return yb ? k_hpsi_pass<R, RZ, MODE, true, false> : k_hpsi_pass<R, RZ, MODE, false, false>;
+}
+
 template <typename R, int RZ, int MODE>
 static cudaError_t launch_pass_t(const System& s, const PassIO& io, int o_beg, int nb, int nbk) {
   PassArgs<R> a;
@@ -444,6 +535,8 @@ static cudaError_t launch_pass_t(const System& s, const PassIO& io, int o_beg, i
     for (int d = 0; d < 3; ++d) {
       a.lapt[4 * d + n] = (R)s.lap[d][n + 1];
       a.nabc[4 * d + n] = (R)s.nab[d][n + 1];
+      a.cl2[4 * d + n] = make_float2((float)s.lap[d][n + 1], (float)s.lap[d][n + 1]);
+      a.cn2[4 * d + n] = make_float2((float)s.nab[d][n + 1], (float)s.nab[d][n + 1]);
     }
   a.sp_off = s.sp_off;
   a.nyblk = s.nyblk;
@@ -457,9 +550,10 @@ static cudaError_t launch_pass_t(const System& s, const PassIO& io, int o_beg, i
   for (int n = 0; n < 4; ++n) a.zf[n] = mk<R>((R)io.zfac[n][0], (R)io.zfac[n][1]);
   const int nthr = a.NYB * (s.NLz / RZ);
   const int block = ((nthr + 31) / 32) * 32;
+  const bool tb = pass_tables(s, RZ);
   const size_t smem = pass_smem_bytes(std::is_same<R, float>::value ? SGPU_PREC_C64 : SGPU_PREC_C128, s.NLy, s.NLz,
-                                      s.maxpts, io.W != nullptr, s.NLx, s.nyblk, a.NYB);
-  auto kern = s.nyblk > 1 ? k_hpsi_pass<R, RZ, MODE, true> : k_hpsi_pass<R, RZ, MODE, false>;
+                                      s.maxpts, io.W != nullptr, s.NLx, s.nyblk, a.NYB, tb);
+  auto kern = pass_kernel<R, RZ, MODE>(s.nyblk > 1, tb);
   if (smem > 48 * 1024) {
     // set outside stream capture (prepare_pass sets it before a capture)
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -496,22 +590,16 @@ cudaError_t launch_hpsi_pass(const System& s, int mode, const PassIO& io, int o_
 
 template <typename R, int RZ>
 static cudaError_t prepare_pass_rz(const System& s) {
+  const bool yb = s.nyblk > 1, tb = pass_tables(s, RZ);
   const size_t smem = pass_smem_bytes(std::is_same<R, float>::value ? SGPU_PREC_C64 : SGPU_PREC_C128, s.NLy, s.NLz,
-                                      s.maxpts, true, s.NLx, s.nyblk, s.nyblk > 1 ? s.NYB : s.NLy);
+                                      s.maxpts, true, s.NLx, s.nyblk, yb ? s.NYB : s.NLy, tb);
   if (smem <= 48 * 1024) return cudaSuccess;
   cudaError_t e;
-  if (s.nyblk > 1) {
-    if ((e = cudaFuncSetAttribute(k_hpsi_pass<R, RZ, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
-      return e;
-    if ((e = cudaFuncSetAttribute(k_hpsi_pass<R, RZ, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
-      return e;
-    return cudaFuncSetAttribute(k_hpsi_pass<R, RZ, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  }
-  if ((e = cudaFuncSetAttribute(k_hpsi_pass<R, RZ, 0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+  if ((e = cudaFuncSetAttribute(pass_kernel<R, RZ, 0>(yb, tb), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
     return e;
-  if ((e = cudaFuncSetAttribute(k_hpsi_pass<R, RZ, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+  if ((e = cudaFuncSetAttribute(pass_kernel<R, RZ, 1>(yb, tb), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
     return e;
-  return cudaFuncSetAttribute(k_hpsi_pass<R, RZ, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return cudaFuncSetAttribute(pass_kernel<R, RZ, 2>(yb, tb), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
 cudaError_t prepare_pass(const System& s) {

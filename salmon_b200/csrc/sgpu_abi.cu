@@ -912,6 +912,11 @@ extern "C" int sgpu_set_param(sgpu_handle h, int param, int value) {
         return fail(SGPU_ERR_ARG, "sgpu_set_param: uvpsi split must be 1, 2, 4 or 8");
       s->um_split = value;
       return 0;
+    case SGPU_PARAM_PASS_TABLES:
+      if (value != 0 && value != 1) return fail(SGPU_ERR_ARG, "sgpu_set_param: pass tables must be 0 or 1");
+      s->pass_tab = value;
+      if (sgpu::prepare_pass(*s) != cudaSuccess) return fail(SGPU_ERR_CUDA, "sgpu_set_param: pass setup failed");
+      return 0;
     case SGPU_PARAM_LAUNCHES:
       if (value != 0) return fail(SGPU_ERR_ARG, "sgpu_set_param: the launch counter can only be reset to 0");
       s->launches = 0;
@@ -928,6 +933,7 @@ extern "C" int sgpu_get_param(sgpu_handle h, int param, int* value) {
     case SGPU_PARAM_LAUNCHES: *value = (int)(h->launches & 0x7fffffffULL); return 0;
     case SGPU_PARAM_UVPSI_SPLIT: *value = h->um_split; return 0;
     case SGPU_PARAM_CG_PRECOND: *value = h->cg_precond; return 0;
+    case SGPU_PARAM_PASS_TABLES: *value = h->pass_tab; return 0;
     default: return fail(SGPU_ERR_ARG, "sgpu_get_param: unknown parameter");
   }
 }

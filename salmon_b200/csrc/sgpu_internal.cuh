@@ -166,6 +166,7 @@ struct System {
   int nslab = 1;                   // x-slabs per orbital in the stencil pass
   int nyblk = 1, NYB = 0;          // y-blocks per plane (planes wider than 512 threads) and their rows
   int* sp_blk = nullptr;           // [NLx*(nyblk+1)] first sphere point of each (plane, y-block)
+  int pass_tab = 1;                // stencil pass: Vloc/sphere-index tables through the ring (two-point form)
   int um_split = 4;                // warps splitting the points of one projection tile (1, 2, 4, 8)
   int cg_precond = 0;              // ground-state CG preconditioner: 0 none, 1 TPA, 2 learned
   double cg_delta = 1e-15;         // CG stops a band when its Rayleigh quotient moves less than this
@@ -196,7 +197,8 @@ cudaError_t launch_kbfield(const System& s, int o_beg, int nb, int nbk, void* W,
 cudaError_t launch_kb_term(const System& s, const void* in, bool from_S, int o_beg, int nb, int nbk, void* W,
                            int prec = -1);
 // dynamic shared memory of the pass kernel
-size_t pass_smem_bytes(int prec, int NLy, int NLz, int maxpts, bool with_w, int NLx, int nyblk = 1, int NYB = 0);
+size_t pass_smem_bytes(int prec, int NLy, int NLz, int maxpts, bool with_w, int NLx, int nyblk = 1, int NYB = 0,
+                       bool tables = false);
 
 // One H application: out = H in  (mode 0), with ttpsi (mode 1), or the last
 // Taylor pass (mode 2): zu = zu + z1 t1 + z2 t2 + z3 in + z4 H in.  U must hold

@@ -163,3 +163,28 @@ def test_errors_are_reported_not_fatal(cuda_lib):
         g.update_projector(kAc)
         with pytest.raises(SalmonGPUError, match="ik outside"):
             g.hpsi_omp_KB_RT(5, zu[0, 0])
+
+
+@pytest.mark.parametrize("nslab", [1, 3])
+@pytest.mark.parametrize("tables", [0, 1])
+@pytest.mark.parametrize("precision", ["c128", "c64"])
+def test_pass_table_staging(case, precision, tables, nslab):
+    """The stencil pass with Vloc and the sphere-index table staged through
+    shared memory (or loaded from global memory one plane ahead), with the
+    orbitals split into x-slabs: H psi, the GS form and a Taylor step against the oracle."""
+    _, sysm, kAc, vloc, zu, zproj = case
+    dt = 0.08
+    tol_h, tol_s = (TOL64, TOL64) if precision == "c128" else (TOL32_HPSI, TOL32_STEP)
+    z0 = zu if precision == "c128" else c64_round(zu)
+    with make_gpu(sysm, kAc, vloc, zu, precision) as g:
+        g.set_param("pass_tables", tables)
+        g.set_param("nslab", min(nslab, sysm.NLx))
+        assert g.get_param("pass_tables") == tables
+        ik = sysm.NK_s
+        t = zu[0, -1]
+        h_ref, tt_ref = O.hpsi(sysm, kAc, vloc, zproj, ik, t, want_tt=True)
+        assert rel(g.hpsi_omp_KB_RT(ik, t), h_ref) < tol_h
+        h2, tt = g.hpsi_omp_KB_GS(ik, t)
+        assert rel(h2, h_ref) < tol_h and rel(tt, tt_ref) < tol_h
+        g.hamiltonian(dt)
+        assert rel(g.get_state(), O.hamiltonian(sysm, kAc, vloc, zproj, dt, z0)) < tol_s
