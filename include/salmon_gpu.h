@@ -276,9 +276,12 @@ enum {
   SGPU_PARAM_LAUNCHES = 1,    /* kernels the handle has launched, modulo 2^31 (read; set 0 to reset) */
   SGPU_PARAM_UVPSI_SPLIT = 2, /* warps splitting the points of one projection tile: 1, 2, 4 or 8     */
   SGPU_PARAM_CG_PRECOND = 3,  /* sgpu_cg direction: SGPU_CG_PLAIN, SGPU_CG_TPA or SGPU_CG_LEARNED     */
-  SGPU_PARAM_PASS_TABLES = 4  /* stencil pass: 1 stages Vloc and the sphere-index table of each plane
+  SGPU_PARAM_PASS_TABLES = 4, /* stencil pass: 1 stages Vloc and the sphere-index table of each plane
                                  through shared memory with the plane (where it fits), 0 loads them
                                  from global memory one plane ahead                                   */
+  SGPU_PARAM_KB_KERNEL = 5    /* KB term of H psi: 1 band-group tile kernel (32 bands of a k-point per
+                                 CTA, pipelined gathers), 2 band-quad kernel (UVPSI_SPLIT warps per
+                                 4 bands), 0 the tile kernel when its grid has >= 2 CTAs per SM       */
 };
 
 /* CG preconditioners.  PLAIN is the reference's CG_ompk.  TPA multiplies the
@@ -297,8 +300,10 @@ int sgpu_get_param(sgpu_handle h, int param, int* value);
 
 /* Autotuner: times `reps` H applications of the resident orbitals (projections,
  * KB field, stencil pass) for every launch shape it knows (x-slabs per orbital
- * 1, 2, 4; projection split 1, 2, 4, 8), keeps the fastest in the handle and
- * returns it (any output pointer may be NULL).  The resident orbitals are not
+ * 1, 2, 4; KB term by the band-group tile kernel, returned as split 0, or by
+ * the band-quad kernel with projection split 1, 2, 4, 8), keeps the fastest in
+ * the handle (SGPU_PARAM_NSLAB, SGPU_PARAM_KB_KERNEL, SGPU_PARAM_UVPSI_SPLIT)
+ * and returns it (any output pointer may be NULL).  The resident orbitals are not
  * modified.  No reference counterpart; the nearest is auto_blocking
  * (modules/opt_variables.f90:340-353). */
 int sgpu_autotune(sgpu_handle h, int reps, int* nslab, int* split, double* ms_per_apply);

@@ -3,6 +3,7 @@
 // Hamiltonian pass itself is in k_pass.cu.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <type_traits>
 
 #include "sgpu_internal.cuh"
@@ -429,6 +430,225 @@ static cudaError_t launch_kb_fused_split(const System& s, const void* in, int ld
   return cudaGetLastError();
 }
 
+// ------------------------------------------------------------ KB tile ---
+// Projections and KB field of one projector item for a group of up to 32
+// bands of one k-point per CTA: U = Hxyz iuV sum_j conj(zproj) in(J(j)), then
+// W = zproj U at the item's single-item points (hpsi.f90:188-206), the
+// contractions on the FP64 tensor pipe as in k_uvpsi / k_kbfield.  The atom's
+// sphere values (gathered by idx) and its zproj rows stream through a
+// three-stage shared-memory pipeline of cp.async copies in chunks of CP points,
+// so several chunks of every CTA are in flight; zproj is read from L2 twice per
+// (k-point, item, band group) instead of twice per band quad.  KBT_KS warps
+// share each band quad (an 8x8 C tile): they split every chunk's points and
+// their tiles are added in warp order, so the sums are deterministic.
+constexpr int KBT_WARPS = 8;               // band quads per CTA
+constexpr int KBT_KS = 2;                  // warps per band quad
+constexpr int KBT_BANDS = 4 * KBT_WARPS;   // bands per CTA
+constexpr int KBT_NS = 3;                  // pipeline stages
+template <typename R>
+struct KbtGeom {
+  static constexpr bool F = std::is_same<R, float>::value;
+  static constexpr int CP = F ? 32 : 16;          // points per chunk
+  static constexpr int SROW = CP + (F ? 4 : 2);   // padded band row of a chunk
+  static constexpr int ZROW = CP + 2;             // padded projector row of a chunk
+  static size_t smem(int Nps) {
+    return sizeof(C2<R>) * (size_t)KBT_NS * KBT_BANDS * SROW + sizeof(double2) * (size_t)KBT_NS * 4 * ZROW +
+           2 * sizeof(int) * (size_t)Nps;
+  }
+};
+
+template <typename R>
+__global__ void __launch_bounds__(32 * KBT_WARPS * KBT_KS) k_kb_tile(const C2<R>* __restrict__ in, int ld_in, int o_beg, int nb,
+                                                          int nbk, int kl0, int ngrp, const double2* __restrict__ zproj,
+                                                          int Nlma, int Nps, const int* __restrict__ idx,
+                                                          const int* __restrict__ kbq, const int* __restrict__ atom_off,
+                                                          const int4* __restrict__ items,
+                                                          const int* __restrict__ lma_list, const int* __restrict__ iuV,
+                                                          double scale, double2* __restrict__ U, int nsp,
+                                                          C2<R>* __restrict__ W) {
+  using T = C2<R>;
+  constexpr int CP = KbtGeom<R>::CP, SROW = KbtGeom<R>::SROW, ZROW = KbtGeom<R>::ZROW;
+  constexpr int NT = 32 * KBT_WARPS * KBT_KS;
+  static_assert(NT % CP == 0 && 4 * CP <= NT, "chunk layout: each thread copies one point of several bands");
+  static_assert((CP / 4) % (2 * KBT_KS) == 0 && (CP / 8) % KBT_KS == 0, "chunk points split evenly over a quad's warps");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* Sb = reinterpret_cast<T*>(smem_raw);                                          // [NS][BANDS][SROW]
+  double2* Zb = reinterpret_cast<double2*>(Sb + (size_t)KBT_NS * KBT_BANDS * SROW);  // [NS][4][ZROW]
+  int* ixs = reinterpret_cast<int*>(Zb + (size_t)KBT_NS * 4 * ZROW);                // [mps] gather index
+  int* kqs = ixs + Nps;                                                              // [mps] W index (-1: multi)
+  __shared__ double2 Us[KBT_WARPS][4][4];  // [quad][projector][band]
+  __shared__ double2 part[KBT_KS][KBT_WARPS][32];
+
+  const int t = threadIdx.x, lane = t & 31;
+  const int warp = (t >> 5) % KBT_WARPS, ks = (t >> 5) / KBT_WARPS;  // band quad, share of the points
+  const int kq = blockIdx.x / ngrp, grp = blockIdx.x - kq * ngrp;
+  const int kl = kl0 + kq;
+  const int o_lo = max(o_beg, kl * nbk + grp * KBT_BANDS);
+  const int o_hi = min(min(o_beg + nb, (kl + 1) * nbk), kl * nbk + (grp + 1) * KBT_BANDS);
+  if (o_lo >= o_hi) return;  // whole CTA leaves together
+  const int nbq = o_hi - o_lo;
+  const int4 item = items[blockIdx.y];
+  const int a = item.x, l0 = item.y, np = item.z;
+  const int p0 = atom_off[a], mps = atom_off[a + 1] - p0;
+  const int nch = (mps + CP - 1) / CP;
+  for (int j = t; j < mps; j += NT) {
+    ixs[j] = __ldg(idx + p0 + j);
+    kqs[j] = __ldg(kbq + p0 + j);
+  }
+  // the copy role of this thread: point jj of a chunk, for bands bc, bc + NT/CP, ...
+  // and (t < 4 CP) projector pz of the zproj rows
+  const int jj = t % CP, bc = t / CP;
+  const int pz = t / CP;
+  const double2* zsrc = (t < 4 * CP && pz < np) ? zproj + ((size_t)kl * Nlma + lma_list[l0 + pz]) * Nps : nullptr;
+  __syncthreads();
+
+  auto issue = [&](int c, bool with_s) {  // chunk c into stage c % NS
+    if (c < nch) {
+      const int s = c % KBT_NS;
+      const int j = c * CP + jj;
+      if (with_s) {
+        T* sd = Sb + (size_t)s * KBT_BANDS * SROW + jj;
+        const int g = j < mps ? ixs[j] : 0;
+#pragma unroll
+        for (int b = bc; b < KBT_BANDS; b += NT / CP) {
+          if (b < nbq && j < mps) {
+            const T* src = in + (size_t)(o_lo + b - o_beg) * ld_in + g;
+            if constexpr (sizeof(T) == 8) cp_async8(sd + b * SROW, src); else cp_async16(sd + b * SROW, src);
+          } else {
+            sd[b * SROW] = mk<R>(0, 0);
+          }
+        }
+      }
+      if (t < 4 * CP) {
+        double2* zd = Zb + (size_t)s * 4 * ZROW + pz * ZROW + jj;
+        if (zsrc && j < mps) cp_async16(zd, zsrc + j); else *zd = make_double2(0.0, 0.0);
+      }
+    }
+    cp_async_commit();
+  };
+
+  // ---- phase 1: the warp's 8x8 tile C = A B over all points (A: zproj rows, B: band values)
+  const int krow = lane & 3, n = lane >> 2;
+  const int pa = n & 3, zpart = n >> 2;                    // A row n: projector n%4, Re (n<4) / Im
+  const int bb = 4 * warp + (n >> 1), bpart = n & 1;       // B column n: band n/2 of the quad, Re/Im
+  double c0 = 0.0, c1 = 0.0, e0 = 0.0, e1 = 0.0;
+  issue(0, true);
+  issue(1, true);
+  for (int c = 0; c < nch; ++c) {
+    cp_async_wait<1>();  // this thread's copies of chunk c have landed
+    __syncthreads();     // ... everyone's; the stage of chunk c-1 is free
+    issue(c + 2, true);
+    const int s = c % KBT_NS;
+    const T* sb = Sb + (size_t)s * KBT_BANDS * SROW + bb * SROW;
+    const double* za = reinterpret_cast<const double*>(Zb + (size_t)s * 4 * ZROW + pa * ZROW) + zpart;
+#pragma unroll
+    for (int u = 2 * ks; u < CP / 4; u += 2 * KBT_KS) {
+      const int j = 4 * u + krow;
+      const T v0 = sb[j], v1 = sb[j + 4];
+      mma_f64_8x8x4(c0, c1, za[2 * j], (double)(bpart ? v0.y : v0.x));
+      mma_f64_8x8x4(e0, e1, za[2 * (j + 4)], (double)(bpart ? v1.y : v1.x));
+    }
+  }
+  part[ks][warp][lane] = make_double2(c0 + e0, c1 + e1);
+  __syncthreads();
+  if (ks == 0) {
+    double x0 = part[0][warp][lane].x, x1 = part[0][warp][lane].y;
+#pragma unroll
+    for (int k2 = 1; k2 < KBT_KS; ++k2) {
+      x0 += part[k2][warp][lane].x;
+      x1 += part[k2][warp][lane].y;
+    }
+    const double d0 = __shfl_down_sync(0xffffffffu, x0, 16);
+    const double d1 = __shfl_down_sync(0xffffffffu, x1, 16);
+    if (lane < 16) {  // C rows p (Re zproj) and p+4 (Im zproj), columns of band bq
+      const int p = lane >> 2, bq = lane & 3, o = o_lo + 4 * warp + bq;
+      double2 u = make_double2(0.0, 0.0);
+      if (p < np && o < o_hi) {
+        const int ilma = lma_list[l0 + p];
+        const double f = scale * (double)iuV[ilma];
+        u = make_double2((x0 + d1) * f, (x1 - d0) * f);
+        U[(size_t)(o - o_beg) * Nlma + ilma] = u;
+      }
+      Us[warp][p][bq] = u;
+    }
+  }
+  __syncthreads();  // Us written; every warp is done with the phase-1 stages
+
+  // ---- phase 2: W = zproj U at the item's single-item points, 8 points per pair of MMAs
+  const int p = krow;  // B row / A column: projector
+  const double2 u = Us[warp][p][n >> 1];
+  const double bre = (n & 1) ? u.y : u.x;   // rows of Re zproj
+  const double bim = (n & 1) ? u.x : -u.y;  // rows of Im zproj
+  const int oc = o_lo + 4 * warp + p;       // the orbital of this lane's C elements
+  const bool cvalid = oc < o_hi;
+  T* Wb = W + (size_t)(cvalid ? oc - o_beg : 0) * nsp;
+  issue(0, false);
+  issue(1, false);
+  for (int c = 0; c < nch; ++c) {
+    cp_async_wait<1>();
+    __syncthreads();
+    issue(c + 2, false);
+    const double2* zb = Zb + (size_t)(c % KBT_NS) * 4 * ZROW + p * ZROW;
+#pragma unroll
+    for (int t8 = ks; t8 < CP / 8; t8 += KBT_KS) {
+      const int jl = 8 * t8 + n, j = c * CP + jl;
+      const double2 z = zb[jl];
+      double w0 = 0.0, w1 = 0.0;
+      mma_f64_8x8x4(w0, w1, z.x, bre);
+      mma_f64_8x8x4(w0, w1, z.y, bim);
+      if (cvalid && j < mps) {
+        const int q = kqs[j];
+        if (q >= 0) Wb[q] = mk<R>((R)w0, (R)w1);
+      }
+    }
+  }
+  cp_async_wait<0>();
+}
+
+template <typename R>
+static cudaError_t launch_kb_tile_t(const System& s, const void* in, int ld_in, const int* idx, int o_beg, int nb,
+                                    int nbk, void* W) {
+  const int kl0 = o_beg / nbk, kl1 = (o_beg + nb - 1) / nbk;
+  const int ngrp = (nbk + KBT_BANDS - 1) / KBT_BANDS;
+  // the kernel's static shared memory counts against the default limit, so the
+  // dynamic limit is raised for every size (once per handle; prepare_kb does it
+  // before a stream capture)
+  const size_t smem = KbtGeom<R>::smem(s.Nps);
+  if (!s.kb_smem_ok) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(s.stream, &cs);
+    if (e != cudaSuccess) return e;
+    if (cs == cudaStreamCaptureStatusNone && (e = prepare_kb(s)) != cudaSuccess) return e;
+  }
+  dim3 grid((kl1 - kl0 + 1) * ngrp, s.nitems);
+  k_kb_tile<R><<<grid, 32 * KBT_WARPS * KBT_KS, smem, s.launch_stream()>>>(
+      (const C2<R>*)in, ld_in, o_beg, nb, nbk, kl0, ngrp, s.zproj64, s.Nlma, s.Nps, idx, s.kbq, s.atom_off, s.items,
+      s.lma_list, s.iuV_d, s.Hxyz, s.U, s.nsp, (C2<R>*)W);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || s.n_multi == 0) return e;
+  dim3 g2((s.n_multi + 255) / 256, (nb + KU - 1) / KU);
+  k_kbfield_multi<R><<<g2, 256, 0, s.launch_stream()>>>(s.U, nb, o_beg, nbk, s.zproj64, s.Nlma, s.Nps, s.rec, s.cont,
+                                                         s.kb_multi, s.n_multi, s.nsp, (C2<R>*)W);
+  return cudaGetLastError();
+}
+
+static int kb_tile_ctas(const System& s, int o_beg, int nb, int nbk) {
+  const int kl0 = o_beg / nbk, kl1 = (o_beg + nb - 1) / nbk;
+  return (kl1 - kl0 + 1) * ((nbk + KBT_BANDS - 1) / KBT_BANDS) * s.nitems;
+}
+
+bool kb_tile_fits(const System& s) {  // dynamic + static shared memory of both precisions' kernels
+  constexpr size_t stat = sizeof(double2) * (KBT_WARPS * 16 + KBT_KS * KBT_WARPS * 32);
+  return KbtGeom<double>::smem(s.Nps) + stat <= 227 * 1024 && KbtGeom<float>::smem(s.Nps) + stat <= 227 * 1024;
+}
+
+cudaError_t prepare_kb(const System& s) {
+  cudaError_t e = raise_smem_limit((const void*)k_kb_tile<float>, KbtGeom<float>::smem(s.Nps));
+  if (e == cudaSuccess) e = raise_smem_limit((const void*)k_kb_tile<double>, KbtGeom<double>::smem(s.Nps));
+  s.kb_smem_ok = e == cudaSuccess;
+  return e;
+}
+
 template <typename R>
 static cudaError_t launch_kb_fused_t(const System& s, const void* in, int ld_in, const int* idx, int o_beg, int nb,
                                      int nbk, void* W) {
@@ -446,7 +666,12 @@ cudaError_t launch_kb_term(const System& s, const void* in, bool from_S, int o_b
   const void* src = from_S ? s.Sbuf : in;
   const int ld = from_S ? s.nsp : s.NL;
   const int* idx = from_S ? s.qmap : s.idx_proj;
-  if ((prec < 0 ? s.prec : prec) == SGPU_PREC_C64) return launch_kb_fused_t<float>(s, src, ld, idx, o_beg, nb, nbk, W);
+  const bool f = (prec < 0 ? s.prec : prec) == SGPU_PREC_C64;
+  const bool tile = kb_tile_fits(s) && (s.kb_kernel == 1 || (s.kb_kernel == 0 && kb_tile_ctas(s, o_beg, nb, nbk) >= 2 * s.nsm));
+  if (tile)
+    return f ? launch_kb_tile_t<float>(s, src, ld, idx, o_beg, nb, nbk, W)
+             : launch_kb_tile_t<double>(s, src, ld, idx, o_beg, nb, nbk, W);
+  if (f) return launch_kb_fused_t<float>(s, src, ld, idx, o_beg, nb, nbk, W);
   return launch_kb_fused_t<double>(s, src, ld, idx, o_beg, nb, nbk, W);
 }
 

@@ -61,22 +61,6 @@ struct PassArgs {
 };
 
 // ------------------------------------------------------------- helpers ---
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
 // asynchronous copy of N complex elements (8- or 16-byte aligned runs)
 template <typename R, int N>
 __device__ __forceinline__ void cp_run(C2<R>* dst, const C2<R>* src) {
@@ -335,7 +319,6 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
     __syncthreads();          // ... and everyone's; the slot of plane x-1 is free
     refill(j + NR - 1);
     const T* pl = ring + (size_t)(j % NR) * RYZ;
-    const bool more = x + 1 < x_end;
     if (act) {
       if constexpr (P == 0) {
         if (j == 0) {
@@ -358,7 +341,7 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
           lq[0] = (int)(short)(v2 & 0xffff);
           lq[RZ - 1] = v2 >> 16;
         }
-      } else if (more) {
+      } else if (x + 1 < x_end) {
 #pragma unroll
         for (int r = 0; r < RZ; ++r) vln[r] = __ldg(a.vloc + pbase + NYZ + r);
         if (with_w || do_export) ld_lq<RZ>(lqn, a.lqi + pbase + NYZ);
@@ -560,7 +543,7 @@ static cudaError_t launch_pass_t(const System& s, const PassIO& io, int o_beg, i
     cudaError_t e = cudaStreamIsCapturing(s.stream, &cs);
     if (e != cudaSuccess) return e;
     if (cs == cudaStreamCaptureStatusNone) {
-      e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      e = raise_smem_limit((const void*)kern, smem);
       if (e != cudaSuccess) return e;
     }
   }
@@ -595,11 +578,11 @@ static cudaError_t prepare_pass_rz(const System& s) {
                                       s.maxpts, true, s.NLx, s.nyblk, yb ? s.NYB : s.NLy, tb);
   if (smem <= 48 * 1024) return cudaSuccess;
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute(pass_kernel<R, RZ, 0>(yb, tb), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+  if ((e = raise_smem_limit((const void*)pass_kernel<R, RZ, 0>(yb, tb), smem)))
     return e;
-  if ((e = cudaFuncSetAttribute(pass_kernel<R, RZ, 1>(yb, tb), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+  if ((e = raise_smem_limit((const void*)pass_kernel<R, RZ, 1>(yb, tb), smem)))
     return e;
-  return cudaFuncSetAttribute(pass_kernel<R, RZ, 2>(yb, tb), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return raise_smem_limit((const void*)pass_kernel<R, RZ, 2>(yb, tb), smem);
 }
 
 cudaError_t prepare_pass(const System& s) {

@@ -172,6 +172,10 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
   if (e != cudaSuccess) { delete s; return cuda_fail(e, "cudaGetDevice"); }
   e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { delete s; return cuda_fail(e, "cudaStreamCreate"); }
+  {
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, dev);
+  }
 
   s->prec = precision;
   s->nyblk = nyblk;
@@ -917,6 +921,10 @@ extern "C" int sgpu_set_param(sgpu_handle h, int param, int value) {
       s->pass_tab = value;
       if (sgpu::prepare_pass(*s) != cudaSuccess) return fail(SGPU_ERR_CUDA, "sgpu_set_param: pass setup failed");
       return 0;
+    case SGPU_PARAM_KB_KERNEL:
+      if (value < 0 || value > 2) return fail(SGPU_ERR_ARG, "sgpu_set_param: KB kernel must be 0, 1 or 2");
+      s->kb_kernel = value;
+      return 0;
     case SGPU_PARAM_LAUNCHES:
       if (value != 0) return fail(SGPU_ERR_ARG, "sgpu_set_param: the launch counter can only be reset to 0");
       s->launches = 0;
@@ -934,6 +942,7 @@ extern "C" int sgpu_get_param(sgpu_handle h, int param, int* value) {
     case SGPU_PARAM_UVPSI_SPLIT: *value = h->um_split; return 0;
     case SGPU_PARAM_CG_PRECOND: *value = h->cg_precond; return 0;
     case SGPU_PARAM_PASS_TABLES: *value = h->pass_tab; return 0;
+    case SGPU_PARAM_KB_KERNEL: *value = h->kb_kernel; return 0;
     default: return fail(SGPU_ERR_ARG, "sgpu_get_param: unknown parameter");
   }
 }
@@ -953,15 +962,17 @@ extern "C" int sgpu_autotune(sgpu_handle h, int reps, int* nslab, int* split, do
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  const int old_slab = s->nslab, old_split = s->um_split;
+  const int old_slab = s->nslab, old_split = s->um_split, old_kb = s->kb_kernel;
   double best = 1e300;
   int bs = old_slab, bk = old_split;
   cudaError_t err = cudaSuccess;
   for (int ns : {1, 2, 4}) {
     if (ns > 1 && s->NLx / ns < 8) continue;
-    for (int sp : {1, 2, 4, 8}) {
+    for (int sp : {0, 1, 2, 4, 8}) {  // 0: the band-group tile kernel
+      if (sp == 0 && !sgpu::kb_tile_fits(*s)) continue;
       s->nslab = ns;
-      s->um_split = sp;
+      s->um_split = sp ? sp : old_split;
+      s->kb_kernel = sp ? 2 : 1;
       err = apply_h(s, 0, io, 0, s->norb, s->NBocc, -1, from_S);  // warm-up
       if (err == cudaSuccess) err = cudaEventRecord(e0, s->stream);
       for (int r = 0; r < reps && err == cudaSuccess; ++r) err = apply_h(s, 0, io, 0, s->norb, s->NBocc, -1, from_S);
@@ -980,10 +991,12 @@ extern "C" int sgpu_autotune(sgpu_handle h, int reps, int* nslab, int* split, do
   if (err != cudaSuccess) {
     s->nslab = old_slab;
     s->um_split = old_split;
+    s->kb_kernel = old_kb;
     return cuda_fail(err, "sgpu_autotune");
   }
   s->nslab = bs;
-  s->um_split = bk;
+  s->um_split = bk ? bk : old_split;
+  s->kb_kernel = bk ? 2 : 1;
   if (nslab) *nslab = bs;
   if (split) *split = bk;
   if (ms) *ms = best;

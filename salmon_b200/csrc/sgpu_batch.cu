@@ -51,8 +51,10 @@ void drop_graph(sgpu_batch* b) {
 int capture(sgpu_batch* b, const double* dt, int nsteps) {
   drop_graph(b);
   cudaError_t e;
-  for (System* s : b->sys)
+  for (System* s : b->sys) {
     if ((e = sgpu::prepare_pass(*s)) != cudaSuccess) return bcuda(e, "sgpu_batch_step: prepare");
+    if ((e = sgpu::prepare_kb(*s)) != cudaSuccess) return bcuda(e, "sgpu_batch_step: prepare");
+  }
   std::vector<unsigned long long> before(b->sys.size());
   for (size_t i = 0; i < b->sys.size(); ++i) before[i] = b->sys[i]->launches;
   if ((e = cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)

@@ -18,6 +18,24 @@ template <> struct C2Of<double> { using type = double2; };
 template <typename R> using C2 = typename C2Of<R>::type;
 
 template <typename R> __host__ __device__ __forceinline__ C2<R> mk(R x, R y) { C2<R> c; c.x = x; c.y = y; return c; }
+// cp.async (sm_80+ asynchronous global -> shared copies)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+
 template <typename T> __host__ __device__ __forceinline__ T cadd(T a, T b) { a.x += b.x; a.y += b.y; return a; }
 template <typename T> __host__ __device__ __forceinline__ T csub(T a, T b) { a.x -= b.x; a.y -= b.y; return a; }
 // a*b
@@ -167,7 +185,10 @@ struct System {
   int nyblk = 1, NYB = 0;          // y-blocks per plane (planes wider than 512 threads) and their rows
   int* sp_blk = nullptr;           // [NLx*(nyblk+1)] first sphere point of each (plane, y-block)
   int pass_tab = 1;                // stencil pass: Vloc/sphere-index tables through the ring (two-point form)
-  int um_split = 4;                // warps splitting the points of one projection tile (1, 2, 4, 8)
+  int nsm = 148;                   // SMs of the device
+  mutable bool kb_smem_ok = false;  // the KB tile kernels' shared-memory limits are raised for this handle
+  int um_split = 4;                // band-quad KB kernel: warps splitting the points of one tile (1, 2, 4, 8)
+  int kb_kernel = 0;               // KB term: 0 auto, 1 band-group tile kernel, 2 band-quad kernel
   int cg_precond = 0;              // ground-state CG preconditioner: 0 none, 1 TPA, 2 learned
   double cg_delta = 1e-15;         // CG stops a band when its Rayleigh quotient moves less than this
   bool net_ready = false;          // a preconditioner network has been loaded
@@ -220,6 +241,17 @@ cudaError_t launch_hpsi_pass(const System& s, int mode, const PassIO& io, int o_
 // Sets the shared-memory attribute of every stencil-pass kernel the handle can
 // launch (needed before capturing its launches into a graph).
 cudaError_t prepare_pass(const System& s);
+cudaError_t prepare_kb(const System& s);
+// Raises a kernel's dynamic shared-memory limit to at least `bytes` (never
+// lowers it, so handles of different sizes sharing a kernel keep working).
+inline cudaError_t raise_smem_limit(const void* func, size_t bytes) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, func);
+  if (e != cudaSuccess) return e;
+  if ((size_t)fa.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
+  return cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}  // shared-memory attribute of the KB tile kernel
+bool kb_tile_fits(const System& s);
 int pass_block_threads(int NLy, int NLz);
 
 // zproj(j,ilma,k) = conj(exp(i kAc.r)) uV(j,ilma)  for the local k-points.

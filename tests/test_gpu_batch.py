@@ -101,8 +101,12 @@ def test_autotune_keeps_results(cuda_lib, precision):
     g0.close()
     (g,) = _open([(sysm, kAc, vloc, zu)], precision)
     nslab, split, ms = g.autotune(reps=2)
-    assert nslab in (1, 2, 4) and split in (1, 2, 4, 8) and ms > 0
-    assert g.get_param("nslab") == nslab and g.get_param("uvpsi_split") == split
+    assert nslab in (1, 2, 4) and split in (0, 1, 2, 4, 8) and ms > 0
+    assert g.get_param("nslab") == nslab
+    if split == 0:  # the band-group tile kernel
+        assert g.get_param("kb_kernel") == 1
+    else:
+        assert g.get_param("kb_kernel") == 2 and g.get_param("uvpsi_split") == split
     np.testing.assert_array_equal(g.get_state(), zu.astype(np.complex64 if precision == "c64" else np.complex128)
                                   .astype(np.complex128))
     g.hamiltonian(0.08)

@@ -188,3 +188,69 @@ def test_pass_table_staging(case, precision, tables, nslab):
         assert rel(h2, h_ref) < tol_h and rel(tt, tt_ref) < tol_h
         g.hamiltonian(dt)
         assert rel(g.get_state(), O.hamiltonian(sysm, kAc, vloc, zproj, dt, z0)) < tol_s
+
+
+def _kb_form_checks(sysm, kAc, vloc, zu, zproj, precision, split):
+    import torch
+    tol_h, tol_s = (TOL64, TOL64) if precision == "c128" else (TOL32_HPSI, TOL32_STEP)
+    z0 = zu if precision == "c128" else c64_round(zu)
+    with make_gpu(sysm, kAc, vloc, zu, precision) as g:
+        if split == 0:
+            g.set_param("kb_kernel", 1)
+        else:
+            g.set_param("kb_kernel", 2)
+            g.set_param("uvpsi_split", split)
+        for ikl in range(sysm.nk_local):
+            ik = sysm.NK_s + ikl
+            t = zu[ikl, -1]
+            assert rel(g.hpsi_omp_KB_RT(ik, t), O.hpsi(sysm, kAc, vloc, zproj, ik, t)) < tol_h
+        if precision == "c128":  # a band range that starts and ends inside k-point blocks
+            flat = zu.reshape(-1, sysm.NL)
+            o0, nb = 1, min(flat.shape[0] - 1, sysm.NBoccmax + 3)
+            src = torch.from_numpy(flat[o0:o0 + nb].copy()).cuda()
+            dst = torch.empty_like(src)
+            torch.cuda.synchronize()
+            g.hpsi_batch(o0 + 1, o0 + nb, src.data_ptr(), dst.data_ptr())  # 1-based, inclusive
+            g.synchronize()
+            out = dst.cpu().numpy()
+            for i in range(nb):
+                o = o0 + i
+                ik = sysm.NK_s + o // sysm.NBoccmax
+                assert rel(out[i], O.hpsi(sysm, kAc, vloc, zproj, ik, flat[o])) < tol_h
+        g.hamiltonian(0.08)
+        assert rel(g.get_state(), O.hamiltonian(sysm, kAc, vloc, zproj, 0.08, z0)) < tol_s
+
+
+@pytest.mark.parametrize("split", [0, 4])
+@pytest.mark.parametrize("precision", ["c128", "c64"])
+def test_kb_forms(case, precision, split):
+    """The KB term of H psi by the band-group tile kernel (split 0: kb_kernel 1)
+    and by the band-quad kernel (kb_kernel 2, split 4): single orbitals, a band range that cuts k-point
+    blocks, and a Taylor step, against the oracle."""
+    _, sysm, kAc, vloc, zu, zproj = case
+    _kb_form_checks(sysm, kAc, vloc, zu, zproj, precision, split)
+
+
+@pytest.mark.parametrize("split", [0, 4])
+@pytest.mark.parametrize("precision", ["c128", "c64"])
+def test_kb_forms_many_bands(cuda_lib, precision, split):
+    """More bands than one tile's 32 (a partial second band group) and three
+    atoms whose spheres overlap."""
+    sysm, kAc, vloc, zu = S.small_system(8, 10, 12, nk=2, nb=37, nat=3, seed=31, Rps=2.2)
+    _, zproj = O.update_projector(sysm, kAc)
+    _kb_form_checks(sysm, kAc, vloc, zu, zproj, precision, split)
+
+
+@pytest.mark.parametrize("precision", ["c128", "c64"])
+def test_kb_tile_32cubed(cuda_lib, precision):
+    """The band-group KB kernel at a production grid (32^3, 8 atoms, ~1000
+    points per sphere: the largest shared-memory tile) against the oracle."""
+    sysm, kAc, vloc, zu = S.microbench_system(32, nk_limit=1, Nb=8)
+    _, zproj = O.update_projector(sysm, kAc)
+    tol = TOL64 if precision == "c128" else TOL32_HPSI
+    with make_gpu(sysm, kAc, vloc, zu, precision) as g:
+        g.set_param("kb_kernel", 1)
+        ik = sysm.NK_s
+        for b in (0, sysm.NBoccmax - 1):
+            t = zu[0, b]
+            assert rel(g.hpsi_omp_KB_RT(ik, t), O.hpsi(sysm, kAc, vloc, zproj, ik, t)) < tol
