@@ -36,9 +36,9 @@ sys.path.insert(0, ROOT)
 METRIC = "RT orbital-updates/s: FP32+FP64-reduce vs FP64 GPU at ΔJ<1e-5; hpsi %HBM peak"
 DT = 0.08
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one stencil-pass launch, per
-# orbital, from the capture in profiles/k_hpsi_pass_k_kb_fused_c64_32cubed_864orb.md
+# orbital, from the capture in profiles/k_hpsi_pass_c64_32cubed_864orb.md
 # (864 orbitals; traffic grows with the orbital count).
-NCU_TRAFFIC_BYTES_PER_ORBITAL = {("stencil_pass", "c64", 32): 536.171264e6 / 864}
+NCU_TRAFFIC_BYTES_PER_ORBITAL = {("stencil_pass", "c64", 32): 536.578816e6 / 864}
 
 
 def parse():
@@ -59,6 +59,8 @@ def parse():
     p.add_argument("--batched-steps", type=int, default=1000)
     p.add_argument("--no-large", action="store_true", help="skip the Si216 48^3 run")
     p.add_argument("--precond", action="store_true", help="also run the Si64 CG preconditioner comparison (minutes)")
+    p.add_argument("--kb-kernel", type=int, default=0, choices=[0, 1, 2],
+                   help="KB term kernel of the main leg: 0 by grid size, 1 band-group tile, 2 band-quad (profiling)")
     return p.parse_args()
 
 
@@ -431,6 +433,7 @@ def main():
         g.set_state(zu)
         g.set_vloc(vloc)
         g.update_projector(kAc)
+        g.set_param("kb_kernel", args.kb_kernel)
         stream = torch.cuda.ExternalStream(g.stream)
         for _ in range(args.warmup):
             g.hamiltonian(DT)
