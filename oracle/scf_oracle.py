@@ -55,3 +55,36 @@ def vloc(rho, vpsl, shape, aL, Hxyz):
     vh = hartree(rho, shape, aL)
     exc, vxc = pz(rho)
     return vh + vpsl + vxc, (0.5 * float(np.dot(vh, rho)) * Hxyz, float(np.dot(exc, rho)) * Hxyz)
+
+
+def gs_exact(sysm, kAc0, vpsl, hpsi_columns, n_iter: int = 20, mixer=None):
+    """Ground-state SCF by exact diagonalisation, the checker of the device's
+    CG-based loop (control/ground_state.f90:100-175 with CG + subspace diag
+    replaced by a full eigendecomposition of H(k) on the grid).
+
+    hpsi_columns(ik, vloc) -> H(k) as an (NL, NL) matrix whose column j is H
+    applied to the j-th grid delta; the static part (H - diag(Vloc)) is built
+    once.  The density of the lowest NBoccmax bands (occ of the system) is mixed
+    by ``mixer`` (a salmon_b200.broyden.Broyden-like object with start/mix);
+    Vloc = Vh + Vpsl + Vexc.  Returns (esp (NK, NB), ddns history)."""
+    from scipy.linalg import eigh
+    NL, NK, NB, nocc = sysm.NL, sysm.NK, sysm.NB, sysm.NBoccmax
+    shape = (sysm.NLx, sysm.NLy, sysm.NLz)
+    nelec = float(np.sum(sysm.occ))
+    h0 = [hpsi_columns(ik, vpsl) - np.diag(vpsl) for ik in range(NK)]
+    rho = np.full(NL, nelec / sysm.aLxyz)
+    mixer.start(rho)
+    v, _ = vloc(rho, vpsl, shape, sysm.aL, sysm.Hxyz)
+    hist = []
+    esp = np.zeros((NK, NB))
+    for _ in range(n_iter):
+        rho_out = np.zeros(NL)
+        for ik in range(NK):
+            w, vec = eigh(h0[ik] + np.diag(v), subset_by_index=[0, NB - 1])
+            esp[ik] = w
+            psi = vec[:, :nocc] / np.sqrt(sysm.Hxyz)
+            rho_out += (np.abs(psi) ** 2) @ sysm.occ[ik, :nocc]
+        hist.append(float(np.abs(rho_out - mixer.rho_in[mixer.iter + 1]).sum() * sysm.Hxyz / nelec))
+        rho = mixer.mix(rho_out)
+        v, _ = vloc(rho, vpsl, shape, sysm.aL, sysm.Hxyz)
+    return esp, hist

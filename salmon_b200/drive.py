@@ -12,7 +12,9 @@ the device, sgpu_update_vloc):
                    midpoint for the Taylor step, then rho -> Vh + Vexc -> Vloc
                    (scf=True), k+A(t+dt) for the current
   ground_state_scf the ground-state loop with the density mixed linearly between
-                   iterations (the reference mixes with Broyden, common/broyden.f90)
+                   iterations
+  gs_scf           the reference's SCF loop: Broyden mixing (common/broyden.f90) and
+                   the 'rho_dne' convergence test (control/ground_state.f90:43-180)
 """
 from __future__ import annotations
 
@@ -84,6 +86,48 @@ def ground_state_scf(g, n_iter: int = 40, ncg: int = 4, mix: float = 0.3):
         g.update_vloc(rho_in)
         history.append((float(esp.sum()), float(esp_var.max()), drho))
     esp = g.subspace_diag()
+    return esp, history
+
+
+def gs_scf(g, sysm, kAc0, vpsl, nscf: int = 100, ncg: int = 5, threshold: float = 1e-9, mixer=None):
+    """The periodic ground-state SCF loop of control/ground_state.f90:43-175 on
+    the device orbitals (the caller loads the initial guess with gs_set_state):
+    Gram-Schmidt, rho_in(1) = rho(psi0), Vloc = Vh + Vpsl + Vexc; then per
+    iteration Gram-Schmidt, subspace diag, Gram-Schmidt, CG(ncg), Gram-Schmidt,
+    rho_out, Broyden mixing (common/broyden.f90) and the new Vloc, until
+    ddns_abs_1e = sum|rho_out - rho_in| Hxyz / Nelec < threshold (the 'rho_dne'
+    criterion, ground_state.f90:180).  A final subspace diag gives the
+    eigenvalues.  Returns (esp (nkl,NB), history) with history[i] =
+    (ddns_abs_1e, max esp_var) of iteration i+1."""
+    from .broyden import Broyden
+    mixer = mixer if mixer is not None else Broyden()
+    nelec = float(np.sum(sysm.occ))
+    g.update_projector(np.ascontiguousarray(kAc0, dtype=np.float64))
+    g.set_vpsl(vpsl)
+    g.gram_schmidt()
+    g.gs_to_rt()
+    rho = g.psi_rho_RT()
+    mixer.start(rho)
+    g.update_vloc(rho)
+    history = []
+    for _ in range(nscf):
+        g.gram_schmidt()
+        g.subspace_diag()
+        g.gram_schmidt()
+        esp_var, _ = g.cg(ncg)
+        g.gram_schmidt()
+        g.gs_to_rt()
+        rho_out = g.psi_rho_RT()
+        rho_in = mixer.rho_in[mixer.iter + 1]
+        ddns = float(np.abs(rho_out - rho_in).sum() * sysm.Hxyz / nelec)
+        rho_new = mixer.mix(rho_out)
+        g.update_vloc(rho_new)
+        history.append((ddns, float(esp_var[:, :sysm.NBoccmax].max())))
+        if ddns < threshold:
+            break
+    esp = g.subspace_diag()
+    g.gram_schmidt()
+    g.gs_to_rt()
     return esp, history
 
 

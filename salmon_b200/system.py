@@ -466,3 +466,41 @@ def small_system(NLx=8, NLy=8, NLz=10, nk=3, nb=4, a=(6.0, 6.5, 7.0), nat=2, see
     zu = rng.standard_normal((nk, nb, NL)) + 1j * rng.standard_normal((nk, nb, NL))
     zu = orthonormalise(zu, Hxyz)
     return sysm, kAc, vloc, zu
+
+
+def si_pp_system(tabs, ncell=(1, 1, 1), grid=(8, 8, 8), nkgrid=(4, 4, 4), NB: int = 32, Nocc: int = 16,
+                 a: float = 10.26, seed: int = SEED, with_orbitals: bool = True):
+    """Diamond-Si supercell with the physical pseudopotential ``tabs``
+    (``pseudo.prepare`` of a KY file): sphere points within the element's Rps
+    (calc_jxyz), uV = spline(udV_l) x Ylm on them (calc_uv), Vpsl from the
+    structure factor (calc_vpsl); NB bands of which the lowest Nocc carry
+    occ = 2/NK (init.f90:91-95).  The shape of SALMON's bulk-Si testsuites
+    (001_bulk_gs, 002_bulk_rt) is the default: 8 atoms, 8^3 grid, 4^3 k, 32 bands.
+    Returns (system, kAc0 (3,NK), Vpsl (NL,), zu_GS (nk,NB,NL) or None); zu_GS
+    is seeded random and orthonormal (the reference's init_wf draws random
+    orbitals too)."""
+    from . import pseudo as P
+    nc = np.asarray(ncell)
+    aL = a * nc.astype(np.float64)
+    NLx, NLy, NLz = grid
+    bl = 2 * np.pi / aL
+    kAc0 = uniform_k_grid(*nkgrid, bl)
+    NK = kAc0.shape[1]
+    occ = np.zeros((NK, NB))
+    occ[:, :Nocc] = 2.0 / NK
+    cells = np.array([[i, j, k] for i in range(nc[0]) for j in range(nc[1]) for k in range(nc[2])])
+    Rion = np.concatenate([(DIAMOND_RED + c) * a for c in cells])
+    rps = tabs.pp.rps
+    Mps, Jxyz, Jxx, Jyy, Jzz, dist = calc_jxyz(NLx, NLy, NLz, aL, Rion, rps)
+    uV, iuV, a_tbl = P.kb_tables(tabs, Mps, dist)
+    vpsl, _, _ = P.calc_vpsl(tabs, NLx, NLy, NLz, aL, Rion)
+    sysm = System(NLx=NLx, NLy=NLy, NLz=NLz, aL=aL, kAc0=kAc0, NB=NB, NBoccmax=Nocc, occ=occ, Rion=Rion, Rps=rps,
+                  Mps=Mps, Jxyz=Jxyz, Jxx=Jxx, Jyy=Jyy, Jzz=Jzz, uV=uV, iuV=iuV, a_tbl=a_tbl)
+    sysm.extra.update(seed=seed, zps=tabs.pp.zps)
+    zu = None
+    if with_orbitals:
+        rng = np.random.default_rng(seed)
+        NL = NLx * NLy * NLz
+        zu = rng.standard_normal((NK, NB, NL)) + 1j * rng.standard_normal((NK, NB, NL))
+        zu = orthonormalise(zu, sysm.Hxyz)
+    return sysm, np.ascontiguousarray(kAc0), vpsl, zu

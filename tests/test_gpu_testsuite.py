@@ -1,0 +1,91 @@
+"""SALMON's bulk-Si testsuites end to end on the GPU, against the reference's own
+verification tables (testsuites/001_bulk_gs/verification, 002_bulk_rt/verification,
+stored in tests/golden/testsuite_si.json).
+
+001_bulk_gs: diamond Si, 8 atoms, a = 10.26 bohr, 8^3 grid, 4^3 k-points, 32 bands
+(16 occupied), the KY pseudopotential testsuites/pseudo/Si_rps.dat with lloc = 2, PZ
+LDA, ncg = 5, Broyden mixing, nscf = 100 iterations.  Checked: eigenvalues of
+bands 15-18 at ik = 1 and 64 (tolerance 1e-3 Ha, the reference's).
+002_bulk_rt: from that ground state, 1200 middle-point Taylor steps of dt = 0.1 under
+an Acos2 pulse (1e12 W/cm^2, 110.3 au, omega 0.05696 Ha, z polarised) with the
+self-consistent Hartree + PZ potential rebuilt every step.  Checked: Jm_z at t = 60 and
+120 au and the excitation energy Eall - Eall0 at t = 60 and 120 au (tolerances of the
+reference's table), for complex(8) orbitals and for complex(4) orbitals with FP64
+reductions.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from _helpers import GOLDEN
+from salmon_b200 import drive, pseudo as P, system as S
+
+pytestmark = pytest.mark.gpu
+
+
+def _suite():
+    with open(os.path.join(GOLDEN, "testsuite_si.json")) as f:
+        return json.load(f)
+
+
+@pytest.fixture(scope="module")
+def ground_state(cuda_lib):
+    from salmon_b200.rt import GpuSystem
+    suite = _suite()
+    inp = suite["inputs"]
+    tabs = P.prepare(P.from_npz(os.path.join(GOLDEN, "si_rps_ky.npz"), lloc=inp["lloc_ps"]))
+    sysm, kAc0, vpsl, zu0 = S.si_pp_system(tabs, grid=tuple(inp["num_rgrid"]), nkgrid=tuple(inp["num_kgrid"]),
+                                           NB=inp["nstate"], Nocc=inp["nelec"] // 2)
+    with GpuSystem(sysm, "c128") as g:
+        g.gs_set_state(zu0)
+        esp, hist = drive.gs_scf(g, sysm, kAc0, vpsl, nscf=inp["nscf"], ncg=inp["ncg"],
+                                 threshold=inp["threshold"])
+        zu = g.get_state()
+    return suite, sysm, kAc0, vpsl, esp, hist, zu
+
+
+def test_gs_eigenvalues_match_001(ground_state):
+    suite, sysm, kAc0, vpsl, esp, hist, zu = ground_state
+    # Bands 16 (occupied) and 17 (empty) lie within 1e-3 Ha of each other at several
+    # k-points, so with occupations fixed by band index the density keeps swapping
+    # between them and ddns stalls near 1e-2 (the CPU oracle's exact-diagonalisation
+    # SCF does the same); the reference's table checks the eigenvalues after its
+    # nscf = 100 iterations, and so does this test.
+    print("SCF iterations", len(hist), "ddns of the last five", [f"{h[0]:.2e}" for h in hist[-5:]])
+    esp_sorted = np.sort(esp, axis=1)
+    for r in suite["001_bulk_gs"]:
+        if r["file"] != "Si_eigen.data" or r["col"] != 2:
+            continue
+        ik, ib = divmod(r["row"], sysm.NB)
+        got = esp_sorted[ik, ib]
+        print(f"{r['label']}: {got:+.6f} (ref {r['value']:+.5f}, tol {r['tol']:.0e})")
+        assert abs(got - r["value"]) <= r["tol"], r["label"]
+
+
+@pytest.mark.parametrize("precision", ["c128", "c64"])
+def test_rt_current_and_energy_match_002(ground_state, precision):
+    from salmon_b200.rt import GpuSystem
+    suite, sysm, kAc0, vpsl, esp, hist, zu = ground_state
+    inp = suite["inputs"]
+    dt, nt = inp["dt"], inp["nt"]
+    # one step past nt: the energy row of step it is taken after that step (control_sc.f90:203-231)
+    Ac = drive.init_Ac(nt + 1, dt, "Acos2", epdir=inp["epdir_re1"], rlaser_int_wcm2=inp["rlaser_int_wcm2_1"],
+                       omega=inp["omega1"], pulse_tw=inp["pulse_tw1"])
+    with GpuSystem(sysm, precision) as g:
+        g.set_state(zu)
+        javt, energies = drive.rt_propagate(g, sysm, kAc0, vpsl, Ac, dt, nt + 1, energy_every=1, scf=True)
+    eall0 = energies[0]
+    for r in suite["002_bulk_rt"]:
+        it = r["row"]
+        if r["file"] == "Si_rt.data" and r["col"] == 15:
+            got = javt[it, 2]
+        elif r["file"] == "Si_rt_energy.data" and r["col"] == 2:
+            it = r["row"] * 10                                   # one row every nstep_energy_calc = 10 steps
+            e_tot = -(Ac[it + 2] - Ac[it]) / (2 * dt)
+            got = energies[it + 1] + sysm.aLxyz * float(e_tot @ e_tot) / (8 * np.pi) - eall0
+        else:
+            continue
+        print(f"{precision} {r['label']}: {got:+.6e} (ref {r['value']:+.4e}, tol {r['tol']:.0e})")
+        assert abs(got - r["value"]) <= r["tol"], (precision, r["label"], got)

@@ -1,0 +1,146 @@
+"""Pseudopotential ingest (KY format), Broyden mixing and the analytic rows of
+SALMON's bulk-Si testsuite verification tables, on the CPU.
+
+Fixtures: tests/golden/si_rps_ky.npz (testsuites/pseudo/Si_rps.dat as parsed) and
+tests/golden/testsuite_si.json (inputs and verification tables of
+testsuites/001_bulk_gs and 002_bulk_rt), made by tests/golden/make_testsuite_golden.py.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from _helpers import GOLDEN
+from salmon_b200 import broyden, drive, pseudo as P, system as S
+
+REF_RPS = "/root/reference/testsuites/pseudo/Si_rps.dat"
+
+
+def _si():
+    return P.from_npz(os.path.join(GOLDEN, "si_rps_ky.npz"), lloc=2)
+
+
+def _suite():
+    with open(os.path.join(GOLDEN, "testsuite_si.json")) as f:
+        return json.load(f)
+
+
+def test_fixture_matches_reader():
+    if not os.path.exists(REF_RPS):
+        pytest.skip("reference tree not present")
+    a = P.read_ps_ky(REF_RPS, lloc=2)
+    b = _si()
+    assert a.mr == b.mr and a.zps == b.zps == 4 and a.mlps == b.mlps == 2
+    assert np.array_equal(a.vpp, b.vpp) and np.array_equal(a.upp, b.upp) and np.array_equal(a.rrc, b.rrc)
+
+
+def test_tables_si():
+    t = P.prepare(_si())
+    # d channel is the local one (lloc_ps = 2): no projector; s and p are
+    assert list(t.inorm) == [1, 1, 0]
+    assert t.anorm[2] == 0.0 and t.anorm[0] > 0 and t.anorm[1] > 0
+    # Rps = 1.2 A; the first radial point beyond it (1-based) and the table rows up to it
+    assert abs(t.pp.rps - 1.2 / P.AU_LENGTH_AA) < 1e-15
+    assert t.pp.nrps == 122 and t.radnl.size == 122 and t.vloctbl.size == 122
+    assert np.all(t.radnl[:-1] <= t.pp.rps) and t.radnl[-1] > t.pp.rps
+    # the local channel approaches -Zps/r at the cut-off
+    assert abs(t.vloctbl[-1] * t.radnl[-1] + 4.0) < 0.05
+
+
+def test_spline_is_natural_cubic():
+    from scipy.interpolate import CubicSpline
+    t = P.prepare(_si())
+    for l in (0, 1):
+        a, b, c, d = P.spline(t.radnl, t.udvtbl[:, l])
+        cs = CubicSpline(t.radnl, t.udvtbl[:, l], bc_type="natural")
+        scale = np.abs(t.udvtbl[:, l]).max()
+        for mine, ref in ((a, cs.c[0]), (b, cs.c[1]), (c, cs.c[2]), (d, cs.c[3])):
+            assert np.abs(mine - ref).max() <= 1e-9 * scale / t.pp.step ** 3
+
+
+def test_kb_tables_and_vpsl_si8():
+    t = P.prepare(_si())
+    sysm, kAc0, vpsl, zu = S.si_pp_system(t, with_orbitals=False)
+    assert list(sysm.Mps) == [27] * 8 and sysm.Nlma == 32
+    assert list(sysm.iuV[:4]) == [1, 1, 1, 1] and list(sysm.a_tbl[:8]) == [1, 1, 1, 1, 2, 2, 2, 2]
+    # projectors of different m on the same atom are orthogonal on a symmetric sphere
+    u = sysm.uV[:4, :27]
+    gram = u @ u.T
+    assert np.abs(gram - np.diag(np.diag(gram))).max() < 1e-12 * np.abs(gram).max()
+    # the FFT evaluation of Vpsl equals the direct G sum of calc_vpsl
+    gx, gy, gz, m0 = P.g_vectors(8, 8, 8, sysm.aL)
+    g2 = gx * gx + gy * gy + gz * gz
+    dv = P.calc_vloc(t, np.sqrt(g2))
+    coul = np.zeros_like(g2)
+    nz = np.arange(g2.size) != m0
+    coul[nz] = 4 * np.pi / g2[nz] * 4
+    vion = sum((dv - coul) * np.exp(-1j * (gx * R[0] + gy * R[1] + gz * R[2])) for R in sysm.Rion) / sysm.aLxyz
+    lx, ly, lz = sysm.grid_coords()
+    h = sysm.H
+    phase = np.exp(1j * (np.outer(lx * h[0], gx) + np.outer(ly * h[1], gy) + np.outer(lz * h[2], gz)))
+    direct = np.real(phase @ vion)
+    assert np.abs(direct - vpsl).max() <= 1e-12 * np.abs(direct).max()
+
+
+def test_broyden_first_step_and_convergence():
+    """On a linear fixed-point problem rho_out = J rho + c with slow modes
+    (eigenvalues of J up to 0.97), the first step is linear mixing and 20
+    Broyden steps beat 20 linear-mixing steps by more than 50x."""
+    rng = np.random.default_rng(3)
+    n = 64
+    q = np.linalg.qr(rng.standard_normal((n, n)))[0]
+    jac = q @ np.diag(rng.uniform(0.5, 0.97, n)) @ q.T
+    fixed = rng.uniform(1.0, 2.0, n)                             # positive, like a density
+    c = fixed - jac @ fixed
+    x0 = np.full(n, 1.5)
+    m = broyden.Broyden()
+    m.start(x0)
+    x = m.mix(jac @ x0 + c)
+    assert np.allclose(x, x0 + 0.75 * (jac @ x0 + c - x0))       # first iteration is linear mixing
+    for _ in range(19):
+        x = m.mix(jac @ x + c)
+    lin = x0.copy()
+    for _ in range(20):
+        lin = lin + 0.75 * (jac @ lin + c - lin)
+    assert np.abs(x - fixed).max() < 2e-2 * np.abs(lin - fixed).max()
+
+
+def _rows(table, fname):
+    return [r for r in table if r["file"] == fname]
+
+
+def test_k_points_and_occupations_match_001():
+    suite = _suite()
+    bl = 2 * np.pi / np.asarray(suite["inputs"]["al"])
+    k = S.uniform_k_grid(4, 4, 4, bl)
+    for r in _rows(suite["001_bulk_gs"], "Si_k.data"):
+        ik, col = r["row"], r["col"]
+        got = 1.0 if col == 4 else k[col - 1, ik] / bl[col - 1]      # kw = 1 (Sym = 1)
+        assert abs(got - r["value"]) <= r["tol"], r["label"]
+    t = P.prepare(_si())
+    sysm, _, _, _ = S.si_pp_system(t, with_orbitals=False)
+    for r in _rows(suite["001_bulk_gs"], "Si_eigen.data"):
+        if r["col"] != 3:
+            continue
+        ik, ib = divmod(r["row"], 32)
+        assert abs(sysm.occ[ik, ib] * sysm.NK - r["value"]) <= r["tol"], r["label"]
+
+
+def test_pulse_matches_002():
+    """Ac_tot and E_tot rows of Si_rt.data: the Acos2 pulse of init_Ac with E = -dA/dt
+    by the central difference of control_sc.f90:218-220."""
+    suite = _suite()
+    inp = suite["inputs"]
+    dt, nt = inp["dt"], inp["nt"]
+    Ac = drive.init_Ac(nt + 1, dt, "Acos2", epdir=inp["epdir_re1"], rlaser_int_wcm2=inp["rlaser_int_wcm2_1"],
+                       omega=inp["omega1"], pulse_tw=inp["pulse_tw1"])
+    for r in _rows(suite["002_bulk_rt"], "Si_rt.data"):
+        it, col = r["row"], r["col"]
+        if col == 9:
+            got = Ac[it + 1, 2]
+        elif col == 12:
+            got = -(Ac[it + 2, 2] - Ac[it, 2]) / (2 * dt)
+        else:
+            continue
+        assert abs(got - r["value"]) <= r["tol"], (r["label"], got)
