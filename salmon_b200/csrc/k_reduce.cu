@@ -3,6 +3,8 @@
 // in a fixed order (no atomics), so results are reproducible run to run.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "sgpu_internal.cuh"
 
 namespace sgpu {
@@ -80,136 +82,313 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double* sh /*[32*NV]*
 
 // ------------------------------------------------------------- current ---
 // Per orbital: jt = sum |psi|^2 (current.f90:182-186) and the current_stencil
-// sums F,G,H = 2 sum Im(conj(psi) sum_n nab_n psi(+n)) (stencil/F90/current.f90).
-template <typename R>
-__global__ void __launch_bounds__(256) k_current_orb(const C2<R>* __restrict__ zu, int NLx, int NLy, int NLz,
-                                                      const double* __restrict__ nab12, double* __restrict__ out) {
+// sums F,G,H = 2 sum Im(conj(psi) sum_n nab_n psi(+n)) (stencil/F90/current.f90),
+// with forward neighbours only (n = 1..4), as the reference's stencil has them.
+//
+// One CTA of NT threads per orbital marches along x.  Thread t owns the plane
+// points t, t+NT, ... (P of them); for each it keeps psi at planes x..x+4 in a
+// register queue (converted to FP64 once, on load), so the x-neighbours cost
+// nothing; plane x is staged in FP64 in shared memory (double-buffered) for the
+// y and z neighbours.  Every element is read from HBM once (the four wrap planes
+// twice) and converted once; the loads run D planes ahead of their use.  Sums are FP64, per thread in plane order, then a
+// fixed-order block sum: out[o][4].
+struct Nab12 {
+  double v[12];  // nabx(1:4), naby(1:4), nabz(1:4): kernel parameters, read from the parameter bank
+};
+
+template <typename R, int NT, int P, int D>
+__global__ void __launch_bounds__(NT, 1) k_current_march(const C2<R>* __restrict__ zu, int NLx, int NLy, int NLz,
+                                                       const Nab12 nab, double* __restrict__ out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int NYZ = NLy * NLz;
+  double2* buf = reinterpret_cast<double2*>(smem_raw);  // [2][NYZ]
   __shared__ double sh[32 * 4];
-  const int o = blockIdx.x, NL = NLx * NLy * NLz;
-  const C2<R>* E = zu + (size_t)o * NL;
+  const int o = blockIdx.x, t = threadIdx.x;
+  const C2<R>* E = zu + (size_t)o * NLx * NYZ;
+  const double* nb = nab.v;
+  int yr[P][4], zi[P][4], own[P];
+  bool ok[P];
+#pragma unroll
+  for (int p = 0; p < P; ++p) {
+    const int i = t + NT * p;
+    ok[p] = i < NYZ;
+    own[p] = ok[p] ? i : 0;
+    const int y = own[p] / NLz, z = own[p] - (own[p] / NLz) * NLz;
+#pragma unroll
+    for (int n = 1; n <= 4; ++n) {
+      int yn = y + n, zn = z + n;
+      while (yn >= NLy) yn -= NLy;
+      while (zn >= NLz) zn -= NLz;
+      yr[p][n - 1] = yn * NLz + z;
+      zi[p][n - 1] = y * NLz + zn;
+    }
+  }
+  double2 q[5][P];  // q[m][p]: plane x+m at point p
+#pragma unroll
+  for (int m = 0; m < 5; ++m) {
+    const int xm = m < NLx ? m : m % NLx;
+#pragma unroll
+    for (int p = 0; p < P; ++p) q[m][p] = ok[p] ? to_d2(__ldg(E + (size_t)xm * NYZ + own[p])) : make_double2(0, 0);
+  }
+  C2<R> nxt[D][P];  // planes x+5 .. x+4+D in flight
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    const int xm = (5 + d) % NLx;
+#pragma unroll
+    for (int p = 0; p < P; ++p) nxt[d][p] = ok[p] ? __ldg(E + (size_t)xm * NYZ + own[p]) : C2<R>{};
+  }
+  // a plane's bytes (bulk L2 prefetch needs 16-byte multiples; 0: no prefetch)
+  const unsigned pf_bytes = ((size_t)NYZ * sizeof(C2<R>)) % 16 == 0 ? (unsigned)(NYZ * sizeof(C2<R>)) : 0u;
+  double v[4] = {0, 0, 0, 0};  // jt, F (x), G (y), H (z)
+  for (int x = 0; x < NLx; ++x) {
+    double2* pl = buf + (size_t)(x & 1) * NYZ;
+#pragma unroll
+    for (int p = 0; p < P; ++p)
+      if (ok[p]) pl[own[p]] = q[0][p];
+    if (t == 0 && pf_bytes) {  // plane x+5+D+4 into L2 for the load issued four steps from now
+      prefetch_l2_bulk(E + (size_t)((x + 9 + D) % NLx) * NYZ, pf_bytes);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      if (!ok[p]) continue;
+      const double2 e = q[0][p];
+      v[0] += e.x * e.x + e.y * e.y;
+      double2 sx = make_double2(0, 0), sy = make_double2(0, 0), sz = make_double2(0, 0);
+#pragma unroll
+      for (int n = 1; n <= 4; ++n) {
+        const double2 ex = q[n][p];
+        const double2 ey = pl[yr[p][n - 1]];
+        const double2 ez = pl[zi[p][n - 1]];
+        sx.x += nb[n - 1] * ex.x; sx.y += nb[n - 1] * ex.y;
+        sy.x += nb[3 + n] * ey.x; sy.y += nb[3 + n] * ey.y;
+        sz.x += nb[7 + n] * ez.x; sz.y += nb[7 + n] * ez.y;
+      }
+      // aimag(conj(e) * s) = e.x s.y - e.y s.x
+      v[1] += e.x * sx.y - e.y * sx.x;
+      v[2] += e.x * sy.y - e.y * sy.x;
+      v[3] += e.x * sz.y - e.y * sz.x;
+    }
+    const int xl = (x + 5 + D) % NLx;  // the plane that enters the pipeline
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      q[0][p] = q[1][p];
+      q[1][p] = q[2][p];
+      q[2][p] = q[3][p];
+      q[3][p] = q[4][p];
+      q[4][p] = ok[p] ? to_d2(nxt[0][p]) : make_double2(0, 0);
+#pragma unroll
+      for (int d = 0; d + 1 < D; ++d) nxt[d][p] = nxt[d + 1][p];
+      nxt[D - 1][p] = ok[p] ? __ldg(E + (size_t)xl * NYZ + own[p]) : C2<R>{};
+    }
+  }
+  block_sum<4>(v, sh);
+  if (t == 0) {
+    out[4 * (size_t)o] = v[0];
+    out[4 * (size_t)o + 1] = v[1];
+    out[4 * (size_t)o + 2] = v[2];
+    out[4 * (size_t)o + 3] = v[3];
+  }
+}
+
+// Planes of more than 1024 points: one CTA per (orbital, x-plane), the
+// neighbours read through L1/L2 (CTAs of one orbital are adjacent in launch
+// order, so the x-planes ahead are L2 hits); part[o][x][4].
+template <typename R>
+__global__ void __launch_bounds__(256, 2) k_current_plane(const C2<R>* __restrict__ zu, int NLx, int NLy, int NLz,
+                                                           const double* __restrict__ nab12, double* __restrict__ part) {
+  __shared__ double sh[32 * 4];
+  const int o = blockIdx.x / NLx, x = blockIdx.x - (blockIdx.x / NLx) * NLx;
+  const int NYZ = NLy * NLz;
+  const C2<R>* E = zu + (size_t)o * NLx * NYZ;
+  const C2<R>* P0 = E + (size_t)x * NYZ;
+  const C2<R>* Px[4];
+#pragma unroll
+  for (int n = 1; n <= 4; ++n) {
+    int xn = x + n;
+    while (xn >= NLx) xn -= NLx;
+    Px[n - 1] = E + (size_t)xn * NYZ;
+  }
   double nb[12];
 #pragma unroll
   for (int k = 0; k < 12; ++k) nb[k] = nab12[k];
-  double v[4] = {0, 0, 0, 0};  // jt, F (x), G (y), H (z)
-  for (int i = threadIdx.x; i < NL; i += blockDim.x) {
-    const int iz = i % NLz, iy = (i / NLz) % NLy, ix = i / (NLy * NLz);
-    const double2 e = to_d2(E[i]);
-    v[0] += e.x * e.x + e.y * e.y;
-    double2 sx = make_double2(0, 0), sy = make_double2(0, 0), sz = make_double2(0, 0);
+  double v[4] = {0, 0, 0, 0};
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int y = warp; y < NLy; y += nw) {
+    int yr[4];
 #pragma unroll
     for (int n = 1; n <= 4; ++n) {
-      const int jx = ix + n >= NLx ? ix + n - NLx : ix + n;
-      const int jy = iy + n >= NLy ? iy + n - NLy : iy + n;
-      const int jz = iz + n >= NLz ? iz + n - NLz : iz + n;
-      const double2 ex = to_d2(E[(jx * NLy + iy) * NLz + iz]);
-      const double2 ey = to_d2(E[(ix * NLy + jy) * NLz + iz]);
-      const double2 ez = to_d2(E[(ix * NLy + iy) * NLz + jz]);
-      sx.x += nb[n - 1] * ex.x; sx.y += nb[n - 1] * ex.y;
-      sy.x += nb[3 + n] * ey.x; sy.y += nb[3 + n] * ey.y;
-      sz.x += nb[7 + n] * ez.x; sz.y += nb[7 + n] * ez.y;
+      int yn = y + n;
+      while (yn >= NLy) yn -= NLy;
+      yr[n - 1] = yn * NLz;
     }
-    // aimag(conj(e) * s) = e.x s.y - e.y s.x
-    v[1] += e.x * sx.y - e.y * sx.x;
-    v[2] += e.x * sy.y - e.y * sy.x;
-    v[3] += e.x * sz.y - e.y * sz.x;
+    for (int z = lane; z < NLz; z += 32) {
+      const int i = y * NLz + z;
+      const double2 e = to_d2(__ldg(P0 + i));
+      v[0] += e.x * e.x + e.y * e.y;
+      double2 sx = make_double2(0, 0), sy = make_double2(0, 0), sz = make_double2(0, 0);
+#pragma unroll
+      for (int n = 1; n <= 4; ++n) {
+        int zn = z + n;
+        while (zn >= NLz) zn -= NLz;
+        const double2 ex = to_d2(__ldg(Px[n - 1] + i));
+        const double2 ey = to_d2(__ldg(P0 + yr[n - 1] + z));
+        const double2 ez = to_d2(__ldg(P0 + y * NLz + zn));
+        sx.x += nb[n - 1] * ex.x; sx.y += nb[n - 1] * ex.y;
+        sy.x += nb[3 + n] * ey.x; sy.y += nb[3 + n] * ey.y;
+        sz.x += nb[7 + n] * ez.x; sz.y += nb[7 + n] * ez.y;
+      }
+      v[1] += e.x * sx.y - e.y * sx.x;
+      v[2] += e.x * sy.y - e.y * sy.x;
+      v[3] += e.x * sz.y - e.y * sz.x;
+    }
   }
   block_sum<4>(v, sh);
   if (threadIdx.x == 0) {
-    out[4 * o + 0] = v[0];
-    out[4 * o + 1] = 2.0 * v[1];
-    out[4 * o + 2] = 2.0 * v[2];
-    out[4 * o + 3] = 2.0 * v[3];
+    double* d = part + ((size_t)o * NLx + x) * 4;
+    d[0] = v[0];
+    d[1] = v[1];
+    d[2] = v[2];
+    d[3] = v[3];
   }
 }
 
 // Weighted projections for the nonlocal current (current.f90:247-265):
 // Uw[o][ilma][w] = sum_j conj(zproj(j,ilma,k)) r_w(j) psi(J(j)), r = (1, x, y, z).
+// psi(J(j)) is read from src[o*ld + idx[j]]: the compact sphere values S with
+// the sphere-point map qmap when they are current, else the orbitals with the
+// grid index idx_proj.
+// One CTA per (projector item, k-point) serves every band of that k-point.
+// Work units are (band, projector) pairs, band-major, one per warp and round;
+// the round's band values at the item's points are gathered into shared memory
+// by all threads (eight loads in flight per thread), the projector rows and
+// positions are read through L1.  Lanes split the points; lane sums are combined
+// by shuffles (fixed order).
 template <typename R>
-__global__ void __launch_bounds__(256) k_uvpsi_w(const C2<R>* __restrict__ zu, int NL, int NBocc,
+__global__ void __launch_bounds__(256, 2) k_uvpsi_w(const C2<R>* __restrict__ src, int ld, int NBocc,
                                                   const double2* __restrict__ zproj, int Nlma, int Nps,
-                                                  const int* __restrict__ idx_proj, const int* __restrict__ atom_off,
+                                                  const int* __restrict__ idx, const int* __restrict__ atom_off,
                                                   const double* __restrict__ rpos, const int4* __restrict__ items,
-                                                  int nitems, const int* __restrict__ lma_list,
+                                                  const int* __restrict__ lma_list, int chunk,
                                                   double2* __restrict__ Uw) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  const int o = blockIdx.x, kl = o / NBocc;
-  for (int it = warp; it < nitems; it += nw) {
-    const int4 item = items[it];
-    const int a = item.x, l0 = item.y, np = item.z;
-    const int p0 = atom_off[a], mps = atom_off[a + 1] - p0;
-    double2 acc[4][4];
+  C2<R>* ps = reinterpret_cast<C2<R>*>(smem_raw);                // [nw][chunk] band values
+  int* is = reinterpret_cast<int*>(ps + (size_t)nw * chunk);     // [chunk]
+  const int4 item = items[blockIdx.x];
+  const int kl = blockIdx.y;
+  const int a = item.x, l0 = item.y, np = item.z;
+  const int p0 = atom_off[a], mps = atom_off[a + 1] - p0;
+  const int bpr = nw / np;                      // bands per round
+  const int nrounds = (NBocc + bpr - 1) / bpr;
+  const int wb = warp / np, wp = warp - wb * np;  // this warp's band slot and projector
+  const bool wact = wb < bpr;
+  const int ilma = lma_list[l0 + (wact ? wp : 0)];
+  const double2* zrow = zproj + ((size_t)kl * Nlma + ilma) * Nps;
+  for (int rd = 0; rd < nrounds; ++rd) {
+    const int b = rd * bpr + wb;
+    const int nbr = min(bpr, NBocc - rd * bpr);
+    double2 acc[4];
 #pragma unroll
-    for (int p = 0; p < 4; ++p)
+    for (int w = 0; w < 4; ++w) acc[w] = make_double2(0, 0);
+    for (int c0 = 0; c0 < mps; c0 += chunk) {
+      const int len = min(chunk, mps - c0);
+      __syncthreads();  // ps / is of the previous chunk or round are no longer read
+      for (int j = threadIdx.x; j < len; j += blockDim.x) is[j] = idx[p0 + c0 + j];
+      __syncthreads();
+      const int tot = nbr * len;
+      for (int q0 = threadIdx.x; q0 < tot; q0 += 8 * blockDim.x) {
+        C2<R> vals[8];
+        int slot[8];
 #pragma unroll
-      for (int w = 0; w < 4; ++w) acc[p][w] = make_double2(0, 0);
-    int ilma[4];
+        for (int u = 0; u < 8; ++u) {
+          const int q = q0 + u * blockDim.x;
+          slot[u] = -1;
+          if (q < tot) {
+            const int bb = q / len, j = q - bb * len;
+            slot[u] = bb * chunk + j;
+            vals[u] = __ldg(src + (size_t)(kl * NBocc + rd * bpr + bb) * ld + is[j]);
+          }
+        }
 #pragma unroll
-    for (int p = 0; p < 4; ++p) ilma[p] = p < np ? lma_list[l0 + p] : 0;
-    for (int j = lane; j < mps; j += 32) {
-      const int gi = idx_proj[p0 + j];
-      const double2 e = to_d2(zu[(size_t)o * NL + gi]);
-      const double* r = rpos + 3 * (size_t)(p0 + j);
-      const double rw[4] = {1.0, r[0], r[1], r[2]};
-#pragma unroll
-      for (int p = 0; p < 4; ++p)
-        if (p < np) {
-          const double2 z = zproj[((size_t)kl * Nlma + ilma[p]) * Nps + j];
+        for (int u = 0; u < 8; ++u)
+          if (slot[u] >= 0) ps[slot[u]] = vals[u];
+      }
+      __syncthreads();
+      if (wact && b < NBocc) {
+        const C2<R>* pw = ps + (size_t)wb * chunk;
+        for (int j = lane; j < len; j += 32) {
+          const double2 e = to_d2(pw[j]);
+          const double2 z = __ldg(zrow + c0 + j);
+          const double* r = rpos + 3 * (size_t)(p0 + c0 + j);
+          const double rw[4] = {1.0, __ldg(r), __ldg(r + 1), __ldg(r + 2)};
           // conj(z) * e
           const double2 ze = make_double2(z.x * e.x + z.y * e.y, z.x * e.y - z.y * e.x);
 #pragma unroll
           for (int w = 0; w < 4; ++w) {
-            acc[p][w].x += rw[w] * ze.x;
-            acc[p][w].y += rw[w] * ze.y;
+            acc[w].x += rw[w] * ze.x;
+            acc[w].y += rw[w] * ze.y;
           }
         }
+      }
     }
-#pragma unroll
-    for (int p = 0; p < 4; ++p)
+    if (wact && b < NBocc) {
 #pragma unroll
       for (int w = 0; w < 4; ++w)
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
-          acc[p][w].x += __shfl_xor_sync(0xffffffffu, acc[p][w].x, off);
-          acc[p][w].y += __shfl_xor_sync(0xffffffffu, acc[p][w].y, off);
+          acc[w].x += __shfl_xor_sync(0xffffffffu, acc[w].x, off);
+          acc[w].y += __shfl_xor_sync(0xffffffffu, acc[w].y, off);
         }
-    if (lane == 0)
+      if (lane == 0)
 #pragma unroll
-      for (int p = 0; p < 4; ++p)
-        if (p < np)
-#pragma unroll
-          for (int w = 0; w < 4; ++w) Uw[((size_t)o * Nlma + ilma[p]) * 4 + w] = acc[p][w];
+        for (int w = 0; w < 4; ++w) Uw[((size_t)(kl * NBocc + b) * Nlma + ilma) * 4 + w] = acc[w];
+    }
   }
 }
 
-// Combines the per-orbital terms exactly as current() does (current.f90:182-273)
-// and sums over orbitals in a fixed order.
-__global__ void k_current_final(const double* __restrict__ orb, const double2* __restrict__ Uw,
-                                const double* __restrict__ occ_o, const double* __restrict__ kAc,
-                                const int* __restrict__ iuV, int norb, int NBocc, int Nlma, double Hxyz,
-                                double IaLxyz, double* __restrict__ jav) {
+// Per orbital, combines the plane sums and the weighted projections exactly as
+// current() does (current.f90:182-273): jo[o][d].
+__global__ void k_current_comb(const double* __restrict__ part, int nx, const double2* __restrict__ Uw,
+                               const double* __restrict__ occ_o, const double* __restrict__ kAc,
+                               const int* __restrict__ iuV, int norb, int NBocc, int Nlma, double Hxyz,
+                               double IaLxyz, double* __restrict__ jo) {
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= norb) return;
+  double v[4] = {0, 0, 0, 0};
+  for (int x = 0; x < nx; ++x) {  // per-orbital rows of partial sums, in order
+    const double* d = part + ((size_t)o * nx + x) * 4;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v[k] += d[k];
+  }
+  const int kl = o / NBocc;
+  const double occ = occ_o[o];
+  double j[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) j[d] = occ * kAc[3 * kl + d] * v[0] + 2.0 * v[1 + d] * occ;
+  double jn[3] = {0, 0, 0};
+  for (int l = 0; l < Nlma; ++l) {
+    const double2* u = Uw + ((size_t)o * Nlma + l) * 4;
+    const double f = Hxyz * (double)iuV[l];
+    const double2 u0 = make_double2(u[0].x * f, u[0].y * f);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double2 ud = make_double2(u[1 + d].x * Hxyz, u[1 + d].y * Hxyz);
+      // aimag(conjg(ud) * u0)
+      jn[d] += occ * IaLxyz * 2.0 * (ud.x * u0.y - ud.y * u0.x);
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) jo[3 * (size_t)o + d] = j[d] * Hxyz * IaLxyz + jn[d];
+}
+
+// sum over orbitals in a fixed order
+__global__ void k_current_sum(const double* __restrict__ jo, int norb, double* __restrict__ jav) {
   __shared__ double sh[32 * 3];
   double v[3] = {0, 0, 0};
   for (int o = threadIdx.x; o < norb; o += blockDim.x) {
-    const int kl = o / NBocc;
-    const double occ = occ_o[o];
-    const double jt = orb[4 * o];
-    double j[3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) j[d] = occ * kAc[3 * kl + d] * jt + orb[4 * o + 1 + d] * occ;
-    double jn[3] = {0, 0, 0};
-    for (int l = 0; l < Nlma; ++l) {
-      const double2* u = Uw + ((size_t)o * Nlma + l) * 4;
-      const double f = Hxyz * (double)iuV[l];
-      const double2 u0 = make_double2(u[0].x * f, u[0].y * f);
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        const double2 ud = make_double2(u[1 + d].x * Hxyz, u[1 + d].y * Hxyz);
-        // aimag(conjg(ud) * u0)
-        jn[d] += occ * IaLxyz * 2.0 * (ud.x * u0.y - ud.y * u0.x);
-      }
-    }
-#pragma unroll
-    for (int d = 0; d < 3; ++d) v[d] += j[d] * Hxyz * IaLxyz + jn[d];
+    for (int d = 0; d < 3; ++d) v[d] += jo[3 * (size_t)o + d];
   }
   block_sum<3>(v, sh);
   if (threadIdx.x == 0) {
@@ -219,43 +398,115 @@ __global__ void k_current_final(const double* __restrict__ orb, const double2* _
   }
 }
 
+// shared memory of k_uvpsi_w for a chunk of n points and 8 warps' band values of e bytes each
+static size_t uvpsi_w_smem(int n, size_t e) { return (size_t)n * (8 * e + sizeof(int)); }
+
+// scratch of launch_current (part [norb][NLx][4], jo [norb][3], 12 coefficients)
+// and of launch_energy (part [norb][NLx][2], eo [norb][2], 25 coefficients)
+size_t current_red_elems(int norb, int NLx) { return (size_t)norb * NLx * 4 + 3 * (size_t)norb + 32; }
+
+template <typename R, int NT, int P, int D>
+static cudaError_t current_march(System& s, const Nab12& nab, double* out) {
+  const size_t smem = 2 * (size_t)s.NLy * s.NLz * sizeof(double2);
+  if (smem > 48 * 1024) {
+    const cudaError_t e =
+        cudaFuncSetAttribute(k_current_march<R, NT, P, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  k_current_march<R, NT, P, D><<<s.norb, NT, smem, s.launch_stream()>>>((const C2<R>*)s.zu, s.NLx, s.NLy, s.NLz, nab,
+                                                                        out);
+  return cudaGetLastError();
+}
+
+// the x-marching form up to 1024 points per plane (one point per thread, up to
+// 1024 threads within 64 registers: the coefficients live in the parameter
+// bank), the plane-parallel form beyond.  Measured at 32^3 x 2048 orbitals
+// (complex(4)): 0.60 ms, against 0.61 ms with 512 threads x 2 points and 0.69 ms
+// with 256 x 4 (spills).
+template <typename R>
+static cudaError_t current_stencil(System& s, const Nab12& nab, const double* nab12, double* part, int& nx) {
+  const int NYZ = s.NLy * s.NLz;
+  nx = 1;
+  if (NYZ <= 256) return current_march<R, 256, 1, 1>(s, nab, part);
+  if (NYZ <= 512) return current_march<R, 512, 1, 1>(s, nab, part);
+  if (NYZ <= 1024) return current_march<R, 1024, 1, 1>(s, nab, part);
+  nx = s.NLx;
+  k_current_plane<R><<<s.norb * s.NLx, 256, 0, s.launch_stream()>>>((const C2<R>*)s.zu, s.NLx, s.NLy, s.NLz, nab12,
+                                                                     part);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_current(System& s, double* jav_dev) {
-  double* orb = s.red;  // [norb][4]
-  if ((size_t)4 * s.norb > s.red_elems) return cudaErrorInvalidValue;
-  double* nab12 = s.red + 4 * (size_t)s.norb;
-  if ((size_t)4 * s.norb + 12 > s.red_elems) return cudaErrorInvalidValue;
+  double* part = s.red;                              // [norb][nx][4]
+  double* jo = part + (size_t)s.norb * s.NLx * 4;    // [norb][3]
+  double* nab12 = jo + 3 * (size_t)s.norb;           // [12]
+  if ((size_t)s.norb * s.NLx * 4 + 3 * (size_t)s.norb + 12 > s.red_elems) return cudaErrorInvalidValue;
   double h[12];
   for (int n = 0; n < 4; ++n)
     for (int d = 0; d < 3; ++d) h[4 * d + n] = s.nab[d][n + 1];
   cudaError_t e = cudaMemcpyAsync(nab12, h, sizeof(h), cudaMemcpyHostToDevice, s.stream);
   if (e != cudaSuccess) return e;
-  if (s.prec == SGPU_PREC_C64) {
-    k_current_orb<float><<<s.norb, 256, 0, s.launch_stream()>>>((const float2*)s.zu, s.NLx, s.NLy, s.NLz, nab12, orb);
-    if (s.Nlma)
-      k_uvpsi_w<float><<<s.norb, 256, 0, s.launch_stream()>>>((const float2*)s.zu, s.NL, s.NBocc, s.zproj64, s.Nlma, s.Nps,
-                                                     s.idx_proj, s.atom_off, s.rpos, s.items, s.nitems, s.lma_list,
-                                                     s.Uw);
-  } else {
-    k_current_orb<double><<<s.norb, 256, 0, s.launch_stream()>>>((const double2*)s.zu, s.NLx, s.NLy, s.NLz, nab12, orb);
-    if (s.Nlma)
-      k_uvpsi_w<double><<<s.norb, 256, 0, s.launch_stream()>>>((const double2*)s.zu, s.NL, s.NBocc, s.zproj64, s.Nlma,
-                                                      s.Nps, s.idx_proj, s.atom_off, s.rpos, s.items, s.nitems,
-                                                      s.lma_list, s.Uw);
+  Nab12 nab;
+  for (int k = 0; k < 12; ++k) nab.v[k] = h[k];
+  int nx = 1;
+  e = s.prec == SGPU_PREC_C64 ? current_stencil<float>(s, nab, nab12, part, nx)
+                              : current_stencil<double>(s, nab, nab12, part, nx);
+  if (e != cudaSuccess) return e;
+  if (s.Nlma && s.nitems) {
+    // chunks of at most 1024 (complex(4)) or 512 (complex(8)) points: 66-68 KB of shared memory per CTA
+    const int chunk = std::min(std::max(s.max_mps, 1), s.prec == SGPU_PREC_C64 ? 1024 : 512);
+    const size_t smem = uvpsi_w_smem(chunk, s.prec == SGPU_PREC_C64 ? sizeof(float2) : sizeof(double2));
+    if (smem > 48 * 1024) {  // set on every call: the attribute is per device
+      e = s.prec == SGPU_PREC_C64
+              ? cudaFuncSetAttribute(k_uvpsi_w<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+              : cudaFuncSetAttribute(k_uvpsi_w<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+    }
+    const dim3 gu(s.nitems, s.nkl);
+    // the compact sphere values are current after every Taylor step: 4x fewer bytes than gathering from zu
+    const bool fromS = s.S_valid && s.Sbuf;
+    const int ld = fromS ? s.nsp : s.NL;
+    const int* idx = fromS ? s.qmap : s.idx_proj;
+    if (s.prec == SGPU_PREC_C64)
+      k_uvpsi_w<float><<<gu, 256, smem, s.launch_stream()>>>(fromS ? (const float2*)s.Sbuf : (const float2*)s.zu, ld,
+                                                              s.NBocc, s.zproj64, s.Nlma, s.Nps, idx, s.atom_off,
+                                                              s.rpos, s.items, s.lma_list, chunk, s.Uw);
+    else
+      k_uvpsi_w<double><<<gu, 256, smem, s.launch_stream()>>>(fromS ? (const double2*)s.Sbuf : (const double2*)s.zu,
+                                                               ld, s.NBocc, s.zproj64, s.Nlma, s.Nps, idx, s.atom_off,
+                                                               s.rpos, s.items, s.lma_list, chunk, s.Uw);
   }
-  k_current_final<<<1, 256, 0, s.launch_stream()>>>(orb, s.Uw, s.occ_o, s.kAc_d, s.iuV_d, s.norb, s.NBocc, s.Nlma, s.Hxyz,
-                                           1.0 / s.aLxyz, jav_dev);
+  k_current_comb<<<(s.norb + 127) / 128, 128, 0, s.launch_stream()>>>(part, nx, s.Uw, s.occ_o, s.kAc_d, s.iuV_d,
+                                                                     s.norb, s.NBocc, s.Nlma, s.Hxyz, 1.0 / s.aLxyz,
+                                                                     jo);
+  k_current_sum<<<1, 256, 0, s.launch_stream()>>>(jo, s.norb, jav_dev);
   return cudaGetLastError();
 }
 
 // -------------------------------------------------------------- energy ---
 // tpsum = sum conj(psi) (lap0_2 psi - 0.5 v - i w)  (stencil/F90/total_energy.f90:93-180)
+// One CTA per (orbital, x-plane), planes of an orbital adjacent in launch
+// order (the neighbour planes are L2 hits), laid out like k_current_plane; the plane's
+// two sums go to part[o][x][2] and are added in plane order by k_energy_comb.
 template <typename R>
-__global__ void __launch_bounds__(256) k_ekin_orb(const C2<R>* __restrict__ zu, int NLx, int NLy, int NLz, int NBocc,
-                                                   const double* __restrict__ kAc, const double* __restrict__ coef,
-                                                   double* __restrict__ out) {
+__global__ void __launch_bounds__(256, 2) k_ekin_plane(const C2<R>* __restrict__ zu, int NLx, int NLy, int NLz,
+                                                        int NBocc, const double* __restrict__ kAc,
+                                                        const double* __restrict__ coef, double* __restrict__ part) {
   __shared__ double sh[32 * 2];
-  const int o = blockIdx.x, NL = NLx * NLy * NLz, kl = o / NBocc;
-  const C2<R>* E = zu + (size_t)o * NL;
+  const int o = blockIdx.x / NLx, x = blockIdx.x - (blockIdx.x / NLx) * NLx, kl = o / NBocc;
+  const int NYZ = NLy * NLz;
+  const C2<R>* E = zu + (size_t)o * NLx * NYZ;
+  const C2<R>* P0 = E + (size_t)x * NYZ;
+  const C2<R>* Pp[4];
+  const C2<R>* Pm[4];
+#pragma unroll
+  for (int n = 1; n <= 4; ++n) {
+    int xp = x + n, xm = x - n;
+    while (xp >= NLx) xp -= NLx;
+    while (xm < 0) xm += NLx;
+    Pp[n - 1] = E + (size_t)xp * NYZ;
+    Pm[n - 1] = E + (size_t)xm * NYZ;
+  }
   // coef: [0] = lap0_2, [1..12] = lapt, [13..24] = nab
   const double A = coef[0];
   double lapt[12], nabt[12];
@@ -265,52 +516,74 @@ __global__ void __launch_bounds__(256) k_ekin_orb(const C2<R>* __restrict__ zu, 
     nabt[n] = kAc[3 * kl + n / 4] * coef[13 + n];
   }
   double v2[2] = {0, 0};
-  for (int i = threadIdx.x; i < NL; i += blockDim.x) {
-    const int iz = i % NLz, iy = (i / NLz) % NLy, ix = i / (NLy * NLz);
-    const double2 e = to_d2(E[i]);
-    double2 v = make_double2(0, 0), w = make_double2(0, 0);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int y = warp; y < NLy; y += nw) {
+    int yp[4], ym[4];
 #pragma unroll
     for (int n = 1; n <= 4; ++n) {
-      const int xp = (ix + n) % NLx, xm = (ix - n + 4 * NLx) % NLx;
-      const int yp = (iy + n) % NLy, ym = (iy - n + 4 * NLy) % NLy;
-      const int zp = (iz + n) % NLz, zm = (iz - n + 4 * NLz) % NLz;
-      const double2 a1 = to_d2(E[(xp * NLy + iy) * NLz + iz]), a2 = to_d2(E[(xm * NLy + iy) * NLz + iz]);
-      const double2 b1 = to_d2(E[(ix * NLy + yp) * NLz + iz]), b2 = to_d2(E[(ix * NLy + ym) * NLz + iz]);
-      const double2 c1 = to_d2(E[(ix * NLy + iy) * NLz + zp]), c2 = to_d2(E[(ix * NLy + iy) * NLz + zm]);
-      v.x += lapt[n - 1] * (a1.x + a2.x) + lapt[3 + n] * (b1.x + b2.x) + lapt[7 + n] * (c1.x + c2.x);
-      v.y += lapt[n - 1] * (a1.y + a2.y) + lapt[3 + n] * (b1.y + b2.y) + lapt[7 + n] * (c1.y + c2.y);
-      w.x += nabt[n - 1] * (a1.x - a2.x) + nabt[3 + n] * (b1.x - b2.x) + nabt[7 + n] * (c1.x - c2.x);
-      w.y += nabt[n - 1] * (a1.y - a2.y) + nabt[3 + n] * (b1.y - b2.y) + nabt[7 + n] * (c1.y - c2.y);
+      int a = y + n, b = y - n;
+      while (a >= NLy) a -= NLy;
+      while (b < 0) b += NLy;
+      yp[n - 1] = a * NLz;
+      ym[n - 1] = b * NLz;
     }
-    // z = A e - 0.5 v - i w ;  F += conj(e) z
-    const double2 z = make_double2(A * e.x - 0.5 * v.x + w.y, A * e.y - 0.5 * v.y - w.x);
-    v2[0] += e.x * z.x + e.y * z.y;
-    v2[1] += e.x * z.y - e.y * z.x;
+    for (int z = lane; z < NLz; z += 32) {
+      const int i = y * NLz + z;
+      const double2 e = to_d2(__ldg(P0 + i));
+      double2 v = make_double2(0, 0), w = make_double2(0, 0);
+#pragma unroll
+      for (int n = 1; n <= 4; ++n) {
+        int zp = z + n, zm = z - n;
+        while (zp >= NLz) zp -= NLz;
+        while (zm < 0) zm += NLz;
+        const double2 a1 = to_d2(__ldg(Pp[n - 1] + i)), a2 = to_d2(__ldg(Pm[n - 1] + i));
+        const double2 b1 = to_d2(__ldg(P0 + yp[n - 1] + z)), b2 = to_d2(__ldg(P0 + ym[n - 1] + z));
+        const double2 c1 = to_d2(__ldg(P0 + y * NLz + zp)), c2 = to_d2(__ldg(P0 + y * NLz + zm));
+        v.x += lapt[n - 1] * (a1.x + a2.x) + lapt[3 + n] * (b1.x + b2.x) + lapt[7 + n] * (c1.x + c2.x);
+        v.y += lapt[n - 1] * (a1.y + a2.y) + lapt[3 + n] * (b1.y + b2.y) + lapt[7 + n] * (c1.y + c2.y);
+        w.x += nabt[n - 1] * (a1.x - a2.x) + nabt[3 + n] * (b1.x - b2.x) + nabt[7 + n] * (c1.x - c2.x);
+        w.y += nabt[n - 1] * (a1.y - a2.y) + nabt[3 + n] * (b1.y - b2.y) + nabt[7 + n] * (c1.y - c2.y);
+      }
+      // z = A e - 0.5 v - i w ;  F += conj(e) z
+      const double2 zz = make_double2(A * e.x - 0.5 * v.x + w.y, A * e.y - 0.5 * v.y - w.x);
+      v2[0] += e.x * zz.x + e.y * zz.y;
+      v2[1] += e.x * zz.y - e.y * zz.x;
+    }
   }
   block_sum<2>(v2, sh);
   if (threadIdx.x == 0) {
-    out[2 * o] = v2[0];
-    out[2 * o + 1] = v2[1];
+    part[((size_t)o * NLx + x) * 2] = v2[0];
+    part[((size_t)o * NLx + x) * 2 + 1] = v2[1];
   }
 }
 
-__global__ void k_energy_final(const double* __restrict__ orb, const double2* __restrict__ U,
-                               const double* __restrict__ occ_o, const double* __restrict__ kAc,
-                               const int* __restrict__ iuV, int norb, int NBocc, int Nlma, double Hxyz,
-                               double* __restrict__ e) {
+// per orbital: occ Re(tpsum) Hxyz + occ |k|^2/2 and occ sum |U|^2 iuV
+__global__ void k_energy_comb(const double* __restrict__ part, int NLx, const double2* __restrict__ U,
+                              const double* __restrict__ occ_o, const double* __restrict__ kAc,
+                              const int* __restrict__ iuV, int norb, int NBocc, int Nlma, double Hxyz,
+                              double* __restrict__ eo) {
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= norb) return;
+  double tr = 0;
+  for (int x = 0; x < NLx; ++x) tr += part[((size_t)o * NLx + x) * 2];
+  const int kl = o / NBocc;
+  const double occ = occ_o[o];
+  const double k2 = kAc[3 * kl] * kAc[3 * kl] + kAc[3 * kl + 1] * kAc[3 * kl + 1] + kAc[3 * kl + 2] * kAc[3 * kl + 2];
+  double en = 0;
+  for (int l = 0; l < Nlma; ++l) {
+    const double2 u = U[(size_t)o * Nlma + l];      // Hxyz * sum uV ekr psi
+    en += occ * (u.x * u.x + u.y * u.y) * (double)iuV[l];
+  }
+  eo[2 * (size_t)o] = occ * tr * Hxyz + occ * k2 / 2.0;   // real part of occ*tpsum*Hxyz + occ*|k|^2/2
+  eo[2 * (size_t)o + 1] = en;
+}
+
+__global__ void k_energy_sum(const double* __restrict__ eo, int norb, double* __restrict__ e) {
   __shared__ double sh[32 * 2];
   double v[2] = {0, 0};
   for (int o = threadIdx.x; o < norb; o += blockDim.x) {
-    const int kl = o / NBocc;
-    const double occ = occ_o[o];
-    const double k2 = kAc[3 * kl] * kAc[3 * kl] + kAc[3 * kl + 1] * kAc[3 * kl + 1] + kAc[3 * kl + 2] * kAc[3 * kl + 2];
-    v[0] += occ * orb[2 * o] * Hxyz + occ * k2 / 2.0;   // real part of occ*tpsum*Hxyz + occ*|k|^2/2
-    double en = 0;
-    for (int l = 0; l < Nlma; ++l) {
-      const double2 u = U[(size_t)o * Nlma + l];      // Hxyz * sum uV ekr psi
-      en += occ * (u.x * u.x + u.y * u.y) * (double)iuV[l];
-    }
-    v[1] += en;
+    v[0] += eo[2 * (size_t)o];
+    v[1] += eo[2 * (size_t)o + 1];
   }
   block_sum<2>(v, sh);
   if (threadIdx.x == 0) {
@@ -320,9 +593,10 @@ __global__ void k_energy_final(const double* __restrict__ orb, const double2* __
 }
 
 cudaError_t launch_energy(System& s, double* e_dev) {
-  if ((size_t)2 * s.norb + 32 > s.red_elems) return cudaErrorInvalidValue;
-  double* orb = s.red;
-  double* coef = s.red + 2 * (size_t)s.norb;
+  double* part = s.red;                                // [norb][NLx][2]
+  double* eo = part + 2 * (size_t)s.norb * s.NLx;      // [norb][2]
+  double* coef = eo + 2 * (size_t)s.norb;              // [25]
+  if (2 * (size_t)s.norb * s.NLx + 2 * (size_t)s.norb + 32 > s.red_elems) return cudaErrorInvalidValue;
   double h[25];
   h[0] = -(s.lap[0][0] + s.lap[1][0] + s.lap[2][0]) * 0.5;
   for (int d = 0; d < 3; ++d)
@@ -332,11 +606,14 @@ cudaError_t launch_energy(System& s, double* e_dev) {
     }
   cudaError_t err = cudaMemcpyAsync(coef, h, sizeof(h), cudaMemcpyHostToDevice, s.stream);
   if (err != cudaSuccess) return err;
+  const int gp = s.norb * s.NLx;
+  const int bt = s.NLy >= 8 ? 256 : 32 * s.NLy;
   if (s.prec == SGPU_PREC_C64)
-    k_ekin_orb<float><<<s.norb, 256, 0, s.launch_stream()>>>((const float2*)s.zu, s.NLx, s.NLy, s.NLz, s.NBocc, s.kAc_d, coef, orb);
+    k_ekin_plane<float><<<gp, bt, 0, s.launch_stream()>>>((const float2*)s.zu, s.NLx, s.NLy, s.NLz, s.NBocc, s.kAc_d,
+                                                          coef, part);
   else
-    k_ekin_orb<double><<<s.norb, 256, 0, s.launch_stream()>>>((const double2*)s.zu, s.NLx, s.NLy, s.NLz, s.NBocc, s.kAc_d, coef,
-                                                     orb);
+    k_ekin_plane<double><<<gp, bt, 0, s.launch_stream()>>>((const double2*)s.zu, s.NLx, s.NLy, s.NLz, s.NBocc, s.kAc_d,
+                                                           coef, part);
   err = cudaGetLastError();
   if (err != cudaSuccess) return err;
   // U = Hxyz * sum conj(zproj) psi = Hxyz * sum uV ekr psi  (total_energy.f90:191-197), FP64 projectors
@@ -344,7 +621,9 @@ cudaError_t launch_energy(System& s, double* e_dev) {
     err = launch_uvpsi(s, s.zu, 0, s.norb, s.NBocc, false);
     if (err != cudaSuccess) return err;
   }
-  k_energy_final<<<1, 256, 0, s.launch_stream()>>>(orb, s.U, s.occ_o, s.kAc_d, s.iuV_d, s.norb, s.NBocc, s.Nlma, s.Hxyz, e_dev);
+  k_energy_comb<<<(s.norb + 127) / 128, 128, 0, s.launch_stream()>>>(part, s.NLx, s.U, s.occ_o, s.kAc_d, s.iuV_d,
+                                                                    s.norb, s.NBocc, s.Nlma, s.Hxyz, eo);
+  k_energy_sum<<<1, 256, 0, s.launch_stream()>>>(eo, s.norb, e_dev);
   return cudaGetLastError();
 }
 

@@ -203,6 +203,7 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
     const int m = d->Mps[a];
     if (m < 0 || m > s->Nps) return bail(fail(SGPU_ERR_ARG, "sgpu_create: Mps out of range"));
     atom_off[a + 1] = atom_off[a] + m;
+    s->max_mps = std::max(s->max_mps, m);
     for (int j = 0; j < m; ++j) {
       const int gi = d->Jxyz[(size_t)a * s->Nps + j] - 1;
       if (gi < 0 || gi >= s->NL) return bail(fail(SGPU_ERR_ARG, "sgpu_create: Jxyz out of range"));
@@ -366,7 +367,8 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
   if ((e = dalloc(&s->vloc64, s->NL)) != cudaSuccess) return bail(cuda_fail(e, "alloc vloc64"));
   if ((e = dalloc(&s->vloc32, s->NL)) != cudaSuccess) return bail(cuda_fail(e, "alloc vloc32"));
   const size_t nchunk = (s->norb + 63) / 64;
-  s->red_elems = std::max<size_t>({nchunk * s->NL, 4 * (size_t)s->norb + 64, (size_t)s->NL + 64});
+  s->red_elems = std::max<size_t>({nchunk * s->NL, 4 * (size_t)s->norb + 64, (size_t)s->NL + 64,
+                                   sgpu::current_red_elems(s->norb, s->NLx)});
   if ((e = dalloc(&s->red, s->red_elems)) != cudaSuccess) return bail(cuda_fail(e, "alloc red"));
   s->red_h_elems = (size_t)s->NL + 64;
   if ((e = cudaMallocHost((void**)&s->red_h, s->red_h_elems * sizeof(double))) != cudaSuccess)

@@ -31,6 +31,11 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
+// hint: bring a contiguous global range into L2 (bulk prefetch; the range must
+// lie inside one allocation, start 16-byte aligned and span a multiple of 16 bytes)
+__device__ __forceinline__ void prefetch_l2_bulk(const void* gmem, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(gmem), "r"(bytes) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
@@ -101,6 +106,7 @@ struct System {
   double H[3] = {0, 0, 0}, aL[3] = {0, 0, 0}, Hxyz = 0, aLxyz = 0;
   double lap[3][5] = {}, nab[3][5] = {};
   int NI = 0, Nps = 0, Nlma = 0, NPI = 0, nitems = 0, ninv = 0;
+  int max_mps = 0;                 // largest sphere of one atom (points)
 
   std::vector<double> occ_h;       // occ(NB,NK)
   std::vector<double> kAc_h;       // last kAc (NK,3)
@@ -266,6 +272,8 @@ cudaError_t launch_r64_to_r32(const double* src, float* dst, size_t n, cudaStrea
 cudaError_t launch_psi_rho(System& s, double* rho_dev);
 // per-orbital current terms and the final jav(3) (device)
 cudaError_t launch_current(System& s, double* jav_dev);
+// reduction scratch (doubles) that launch_current and launch_energy need
+size_t current_red_elems(int norb, int NLx);
 // per-orbital kinetic and nonlocal energies summed (device, 2 doubles)
 cudaError_t launch_energy(System& s, double* e_dev);
 
