@@ -279,9 +279,12 @@ enum {
   SGPU_PARAM_PASS_TABLES = 4, /* stencil pass: 1 stages Vloc and the sphere-index table of each plane
                                  through shared memory with the plane (where it fits), 0 loads them
                                  from global memory one plane ahead                                   */
-  SGPU_PARAM_KB_KERNEL = 5    /* KB term of H psi: 1 band-group tile kernel (32 bands of a k-point per
+  SGPU_PARAM_KB_KERNEL = 5,   /* KB term of H psi: 1 band-group tile kernel (32 bands of a k-point per
                                  CTA, pipelined gathers), 2 band-quad kernel (UVPSI_SPLIT warps per
                                  4 bands), 0 the tile kernel when its grid has >= 2 CTAs per SM       */
+  SGPU_PARAM_PASS_FIXED = 6   /* stencil pass, complex(4): 1 uses the compile-time plane shapes
+                                 (16x16, 16x32, 20x20, 32x32 planes: 9-plane ring, constant offsets)
+                                 where they fit, 0 the generic kernel                                 */
 };
 
 /* CG preconditioners.  PLAIN is the reference's CG_ompk.  TPA multiplies the

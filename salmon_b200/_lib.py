@@ -64,7 +64,8 @@ ABI = {
     "sgpu_batch_destroy": (C.c_int, [_vp]),
 }
 
-PARAMS = {"nslab": 0, "launches": 1, "uvpsi_split": 2, "cg_precond": 3, "pass_tables": 4, "kb_kernel": 5}
+PARAMS = {"nslab": 0, "launches": 1, "uvpsi_split": 2, "cg_precond": 3, "pass_tables": 4, "kb_kernel": 5,
+          "pass_fixed": 6}
 
 KERNELS = {"stencil_pass": 0, "taylor_last": 1, "uvpsi": 2, "psi_rho": 3, "kb_field": 4, "kb_term": 5}
 

@@ -159,9 +159,9 @@ template <typename R> struct PassGeom {
 };
 
 size_t pass_smem_bytes(int prec, int NLy, int NLz, int maxpts, bool with_w, int NLx, int nyblk, int NYB,
-                       bool tables) {
+                       bool tables, int nr) {
   const size_t e = prec == SGPU_PREC_C64 ? sizeof(float2) : sizeof(double2);
-  const int NR = prec == SGPU_PREC_C64 ? PassGeom<float>::NR : PassGeom<double>::NR;
+  const int NR = nr > 0 ? nr : (prec == SGPU_PREC_C64 ? PassGeom<float>::NR : PassGeom<double>::NR);
   const size_t ryz = nyblk > 1 ? (size_t)(NYB + 8) * NLz : (size_t)NLy * NLz;
   const size_t tyz = nyblk > 1 ? (size_t)NYB * NLz : (size_t)NLy * NLz;
   return e * (size_t)NR * (ryz + (with_w ? (size_t)maxpts : 0)) +
@@ -178,13 +178,20 @@ size_t pass_smem_bytes(int prec, int NLy, int NLz, int maxpts, bool with_w, int 
 // travel with the plane through the ring (copy group of the plane) instead of
 // being loaded from global memory one plane ahead; this takes the dependent
 // global loads off each march step.
-template <typename R, int RZ, int MODE, bool YB, bool TB>
+//
+// GY, GZ (non-zero: the plane shape NLy x NLz at compile time, complex(4), two-point
+// table form without y-blocks): the ring then has one slot per unrolled phase (NR = 9),
+// so every ring, table and neighbour offset is a compile-time constant and the
+// per-step address arithmetic drops to a few adds.
+template <typename R, int RZ, int MODE, bool YB, bool TB, int GY = 0, int GZ = 0>
 __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
   static_assert(!TB || RZ == 2, "table staging copies the two points' entries as one run");
+  static_assert(GZ == 0 || (std::is_same<R, float>::value && TB && !YB), "fixed shapes: complex(4) table form");
   using T = C2<R>;
-  constexpr int NR = PassGeom<R>::NR;
+  constexpr bool FIXED = GZ > 0;
+  constexpr int NR = FIXED ? 9 : PassGeom<R>::NR;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int NLy = a.NLy, NLz = a.NLz, NYZ = NLy * NLz;
+  const int NLy = FIXED ? GY : a.NLy, NLz = FIXED ? GZ : a.NLz, NYZ = NLy * NLz;
   const bool with_w = a.W != nullptr;
   const bool do_export = a.S != nullptr;
   const int nyblk = YB ? a.nyblk : 1;
@@ -244,13 +251,13 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
   const T* Wb = with_w ? a.W + (size_t)b * a.nsp : nullptr;
   T* Sb = do_export ? a.S + (size_t)b * a.nsp : nullptr;
 
-  // plane jn (relative to x_beg) into ring slot jn % NR, with its W chunk
-  auto refill = [&](int jn) {
+  // plane jn (relative to x_beg) into ring slot sl (= jn modulo the ring), with its W chunk
+  auto refill = [&](int jn, int sl) {
     int p = x_beg + jn;
     while (p >= a.NLx) p -= a.NLx;
     if constexpr (YB) {
       if (jn < nplanes) {  // the block's rows and the halo rows, periodic in y
-        T* dst = ring + (size_t)(jn % NR) * RYZ;
+        T* dst = ring + (size_t)sl * RYZ;
         const T* src = inb + (size_t)p * NYZ;
         for (int idx = t; idx < (a.NYB + 8) * NZG; idx += bd) {
           const int r = idx / NZG, zz = (idx - r * NZG) * RZ;
@@ -261,26 +268,26 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
         }
       }
     } else {
-      if (act && jn < nplanes) cp_run<R, RZ>(ring + (size_t)(jn % NR) * NYZ + own, inb + (size_t)p * NYZ + own);
+      if (act && jn < nplanes) cp_run<R, RZ>(ring + (size_t)sl * NYZ + own, inb + (size_t)p * NYZ + own);
     }
     if constexpr (TB) {
       if (act && jn < nown) {
         const size_t g = (size_t)p * NYZ + own;
-        R* vd = vtab + (size_t)(jn % NR) * TYZ + own_t;
+        R* vd = vtab + (size_t)sl * TYZ + own_t;
         if constexpr (sizeof(R) == 4) cp_async8(vd, a.vloc + g); else cp_async16(vd, a.vloc + g);
-        if (with_w || do_export) cp_async4(lqtab + (size_t)(jn % NR) * TYZ + own_t, a.lqi + g);
+        if (with_w || do_export) cp_async4(lqtab + (size_t)sl * TYZ + own_t, a.lqi + g);
       }
     }
     if (with_w && jn < nown) {
       const int q0 = YB ? spo[p * (nyblk + 1) + yb] : spo[p];
       const int q1 = YB ? spo[p * (nyblk + 1) + yb + 1] : spo[p + 1];
-      T* dst = wring + (size_t)(jn % NR) * a.maxpts;
+      T* dst = wring + (size_t)sl * a.maxpts;
       for (int qq = q0 + t; qq < q1; qq += bd) cp_run<R, 1>(dst + (qq - q0), Wb + qq);
     }
     cp_async_commit();
   };
 #pragma unroll 1
-  for (int n = 0; n < NR - 1; ++n) refill(n);
+  for (int n = 0; n < NR - 1; ++n) refill(n, n);
 
   int yo[8];  // ring offsets of the y neighbours
 #pragma unroll
@@ -315,10 +322,13 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
   auto step = [&](auto phase) -> bool {
     constexpr int P = decltype(phase)::value;
     const int j = x - x_beg;
+    // ring slot of plane j+k: with one slot per phase (j modulo 9 is P) a constant
+    auto slot = [&](int k) -> int { return FIXED ? (P + k) % NR : (j + k) % NR; };
+    const int s0 = slot(0);
     cp_async_wait<NR - 6>();  // this thread's copies of planes <= x+4 have landed
     __syncthreads();          // ... and everyone's; the slot of plane x-1 is free
-    refill(j + NR - 1);
-    const T* pl = ring + (size_t)(j % NR) * RYZ;
+    refill(j + NR - 1, slot(NR - 1));
+    const T* pl = ring + (size_t)s0 * RYZ;
     if (act) {
       if constexpr (P == 0) {
         if (j == 0) {
@@ -326,18 +336,18 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
           for (int n = 4; n < 8; ++n) lds_run<R, RZ>(q[n], ring + (size_t)(n - 4) * RYZ + own_r);
         }
       }
-      lds_run<R, RZ>(q[(P + 8) % 9], ring + (size_t)((j + 4) % NR) * RYZ + own_r);
+      lds_run<R, RZ>(q[(P + 8) % 9], ring + (size_t)slot(4) * RYZ + own_r);
       const size_t pbase = (size_t)x * NYZ + own;
       R vln[RZ];
       int lqn[RZ];
 #pragma unroll
       for (int r = 0; r < RZ; ++r) { vln[r] = (R)0; lqn[r] = -1; }
       if constexpr (TB) {  // this plane's tables arrived with it (copy group j)
-        const R* vs = vtab + (size_t)(j % NR) * TYZ + own_t;
+        const R* vs = vtab + (size_t)s0 * TYZ + own_t;
 #pragma unroll
         for (int r = 0; r < RZ; ++r) vl[r] = vs[r];
         if (with_w || do_export) {
-          const int v2 = *reinterpret_cast<const int*>(lqtab + (size_t)(j % NR) * TYZ + own_t);
+          const int v2 = *reinterpret_cast<const int*>(lqtab + (size_t)s0 * TYZ + own_t);
           lq[0] = (int)(short)(v2 & 0xffff);
           lq[RZ - 1] = v2 >> 16;
         }
@@ -416,7 +426,7 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
       for (int r = 0; r < RZ; ++r) w[r] = kscale(kx, wa[r], w[r]);
 
       // plane-relative sphere index lq -> this block's W chunk
-      const T* wpl = wring + (size_t)(j % NR) * a.maxpts -
+      const T* wpl = wring + (size_t)s0 * a.maxpts -
                      (YB ? spo[x * (nyblk + 1) + yb] - spo[x * (nyblk + 1)] : 0);
       T res[RZ];
 #pragma unroll
@@ -489,12 +499,44 @@ static bool pass_tables(const System& s, int RZ) {
   return true;
 }
 
+// plane shapes with a compile-time form (complex(4), table form, no y-blocks):
+// the 16^3, 20^3 and 32^3 grids and the 16x16x32 supercell
+static int fixed_shape(int NLy, int NLz) {
+  if (NLy == 32 && NLz == 32) return 1;
+  if (NLy == 16 && NLz == 16) return 2;
+  if (NLy == 16 && NLz == 32) return 3;
+  if (NLy == 20 && NLz == 20) return 4;
+  return 0;
+}
+
 template <typename R, int RZ, int MODE>
-static void (*pass_kernel(bool yb, bool tb))(const PassArgs<R>) {
+static void (*pass_kernel(bool yb, bool tb, int shape))(const PassArgs<R>) {
+  if constexpr (RZ == 2 && std::is_same<R, float>::value) {
+    if (tb && !yb) {
+      switch (shape) {
+        case 1: return k_hpsi_pass<R, RZ, MODE, false, true, 32, 32>;
+        case 2: return k_hpsi_pass<R, RZ, MODE, false, true, 16, 16>;
+        case 3: return k_hpsi_pass<R, RZ, MODE, false, true, 16, 32>;
+        case 4: return k_hpsi_pass<R, RZ, MODE, false, true, 20, 20>;
+        default: break;
+      }
+    }
+  }
   if constexpr (RZ == 2) {
     if (tb) return yb ? k_hpsi_pass<R, RZ, MODE, true, true> : k_hpsi_pass<R, RZ, MODE, false, true>;
   }
   return yb ? k_hpsi_pass<R, RZ, MODE, true, false> : k_hpsi_pass<R, RZ, MODE, false, false>;
+}
+
+// the compile-time shape the pass uses for this system and precision (0: none);
+// its 9-plane ring must fit in shared memory
+template <typename R, int RZ>
+static int pass_shape(const System& s, bool tb) {
+  if (!std::is_same<R, float>::value || RZ != 2 || !tb || s.nyblk > 1 || !s.pass_fixed) return 0;
+  const int sh = fixed_shape(s.NLy, s.NLz);
+  if (sh && pass_smem_bytes(SGPU_PREC_C64, s.NLy, s.NLz, s.maxpts, true, s.NLx, 1, s.NLy, true, 9) > 227 * 1024)
+    return 0;
+  return sh;
 }
 
 template <typename R, int RZ, int MODE>
@@ -534,9 +576,10 @@ static cudaError_t launch_pass_t(const System& s, const PassIO& io, int o_beg, i
   const int nthr = a.NYB * (s.NLz / RZ);
   const int block = ((nthr + 31) / 32) * 32;
   const bool tb = pass_tables(s, RZ);
+  const int shape = pass_shape<R, RZ>(s, tb);
   const size_t smem = pass_smem_bytes(std::is_same<R, float>::value ? SGPU_PREC_C64 : SGPU_PREC_C128, s.NLy, s.NLz,
-                                      s.maxpts, io.W != nullptr, s.NLx, s.nyblk, a.NYB, tb);
-  auto kern = pass_kernel<R, RZ, MODE>(s.nyblk > 1, tb);
+                                      s.maxpts, io.W != nullptr, s.NLx, s.nyblk, a.NYB, tb, shape ? 9 : 0);
+  auto kern = pass_kernel<R, RZ, MODE>(s.nyblk > 1, tb, shape);
   if (smem > 48 * 1024) {
     // set outside stream capture (prepare_pass sets it before a capture)
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -574,15 +617,16 @@ cudaError_t launch_hpsi_pass(const System& s, int mode, const PassIO& io, int o_
 template <typename R, int RZ>
 static cudaError_t prepare_pass_rz(const System& s) {
   const bool yb = s.nyblk > 1, tb = pass_tables(s, RZ);
+  const int shape = pass_shape<R, RZ>(s, tb);
   const size_t smem = pass_smem_bytes(std::is_same<R, float>::value ? SGPU_PREC_C64 : SGPU_PREC_C128, s.NLy, s.NLz,
-                                      s.maxpts, true, s.NLx, s.nyblk, yb ? s.NYB : s.NLy, tb);
+                                      s.maxpts, true, s.NLx, s.nyblk, yb ? s.NYB : s.NLy, tb, shape ? 9 : 0);
   if (smem <= 48 * 1024) return cudaSuccess;
   cudaError_t e;
-  if ((e = raise_smem_limit((const void*)pass_kernel<R, RZ, 0>(yb, tb), smem)))
+  if ((e = raise_smem_limit((const void*)pass_kernel<R, RZ, 0>(yb, tb, shape), smem)))
     return e;
-  if ((e = raise_smem_limit((const void*)pass_kernel<R, RZ, 1>(yb, tb), smem)))
+  if ((e = raise_smem_limit((const void*)pass_kernel<R, RZ, 1>(yb, tb, shape), smem)))
     return e;
-  return raise_smem_limit((const void*)pass_kernel<R, RZ, 2>(yb, tb), smem);
+  return raise_smem_limit((const void*)pass_kernel<R, RZ, 2>(yb, tb, shape), smem);
 }
 
 cudaError_t prepare_pass(const System& s) {

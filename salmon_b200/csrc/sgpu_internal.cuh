@@ -191,6 +191,7 @@ struct System {
   int nyblk = 1, NYB = 0;          // y-blocks per plane (planes wider than 512 threads) and their rows
   int* sp_blk = nullptr;           // [NLx*(nyblk+1)] first sphere point of each (plane, y-block)
   int pass_tab = 1;                // stencil pass: Vloc/sphere-index tables through the ring (two-point form)
+  int pass_fixed = 1;              // stencil pass: compile-time plane shapes with a 9-plane ring (complex(4))
   int nsm = 148;                   // SMs of the device
   mutable bool kb_smem_ok = false;  // the KB tile kernels' shared-memory limits are raised for this handle
   int um_split = 4;                // band-quad KB kernel: warps splitting the points of one tile (1, 2, 4, 8)
@@ -224,8 +225,9 @@ cudaError_t launch_kbfield(const System& s, int o_beg, int nb, int nbk, void* W,
 cudaError_t launch_kb_term(const System& s, const void* in, bool from_S, int o_beg, int nb, int nbk, void* W,
                            int prec = -1);
 // dynamic shared memory of the pass kernel
+// (nr: ring planes, 0 = the precision's default)
 size_t pass_smem_bytes(int prec, int NLy, int NLz, int maxpts, bool with_w, int NLx, int nyblk = 1, int NYB = 0,
-                       bool tables = false);
+                       bool tables = false, int nr = 0);
 
 // One H application: out = H in  (mode 0), with ttpsi (mode 1), or the last
 // Taylor pass (mode 2): zu = zu + z1 t1 + z2 t2 + z3 in + z4 H in.  U must hold
