@@ -36,9 +36,9 @@ sys.path.insert(0, ROOT)
 METRIC = "RT orbital-updates/s: FP32+FP64-reduce vs FP64 GPU at ΔJ<1e-5; hpsi %HBM peak"
 DT = 0.08
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one stencil-pass launch, per
-# orbital, from the capture in profiles/k_hpsi_pass_c64_32cubed_864orb.md
+# orbital, from the capture in profiles/k_hpsi_pass_fixed32_c64_32cubed_864orb.md
 # (864 orbitals; traffic grows with the orbital count).
-NCU_TRAFFIC_BYTES_PER_ORBITAL = {("stencil_pass", "c64", 32): 536.578816e6 / 864}
+NCU_TRAFFIC_BYTES_PER_ORBITAL = {("stencil_pass", "c64", 32): 534.936064e6 / 864}
 
 
 def parse():
@@ -59,6 +59,8 @@ def parse():
     p.add_argument("--batched-steps", type=int, default=1000)
     p.add_argument("--no-large", action="store_true", help="skip the Si216 48^3 run")
     p.add_argument("--precond", action="store_true", help="also run the Si64 CG preconditioner comparison (minutes)")
+    p.add_argument("--profile-current", action="store_true",
+                   help="profiling: one complex(4) Taylor step of the workload, then two sgpu_current calls, and exit")
     p.add_argument("--kb-kernel", type=int, default=0, choices=[0, 1, 2],
                    help="KB term kernel of the main leg: 0 by grid size, 1 band-group tile, 2 band-quad (profiling)")
     return p.parse_args()
@@ -409,6 +411,16 @@ def main():
 
     sysm, kAc, vloc, zu = make_workload(args, rank, world)
     norb = sysm.nk_local * sysm.NBoccmax
+    if args.profile_current:  # the current path as the end-to-end leg runs it (sphere values current)
+        with GpuSystem(sysm, "c64") as g:
+            g.set_state(zu)
+            g.set_vloc(vloc)
+            g.update_projector(kAc)
+            g.hamiltonian(DT)
+            for _ in range(2):
+                g.current_RT(kAc)
+            g.synchronize()
+        return
     NL = sysm.NL
     hbm_peak, peak_kind = measured_peaks()
     res = {}
