@@ -20,7 +20,7 @@ import numpy as np
 import pytest
 
 from _helpers import GOLDEN
-from salmon_b200 import drive, pseudo as P, system as S
+from salmon_b200 import drive, outputs as OUT, pseudo as P, system as S
 
 pytestmark = pytest.mark.gpu
 
@@ -46,7 +46,19 @@ def ground_state(cuda_lib):
     return suite, sysm, kAc0, vpsl, esp, hist, zu
 
 
-def test_gs_eigenvalues_match_001(ground_state):
+def _check_table(table, folder, tag=""):
+    """The reference's verification rule on the files a run wrote: np.loadtxt of
+    each file, the value at (row, col) within the tolerance."""
+    data = {}
+    for r in table:
+        if r["file"] not in data:
+            data[r["file"]] = np.loadtxt(os.path.join(folder, r["file"]))
+        got = data[r["file"]][r["row"], r["col"]]
+        print(f"{tag}{r['label']}: {got:+.6e} (ref {r['value']:+.4e}, tol {r['tol']:.0e})")
+        assert abs(got - r["value"]) <= r["tol"], (tag, r["label"], got)
+
+
+def test_gs_eigenvalues_match_001(ground_state, tmp_path):
     suite, sysm, kAc0, vpsl, esp, hist, zu = ground_state
     # Bands 16 (occupied) and 17 (empty) lie within 1e-3 Ha of each other at several
     # k-points, so with occupations fixed by band index the density keeps swapping
@@ -54,18 +66,14 @@ def test_gs_eigenvalues_match_001(ground_state):
     # SCF does the same); the reference's table checks the eigenvalues after its
     # nscf = 100 iterations, and so does this test.
     print("SCF iterations", len(hist), "ddns of the last five", [f"{h[0]:.2e}" for h in hist[-5:]])
-    esp_sorted = np.sort(esp, axis=1)
-    for r in suite["001_bulk_gs"]:
-        if r["file"] != "Si_eigen.data" or r["col"] != 2:
-            continue
-        ik, ib = divmod(r["row"], sysm.NB)
-        got = esp_sorted[ik, ib]
-        print(f"{r['label']}: {got:+.6f} (ref {r['value']:+.5f}, tol {r['tol']:.0e})")
-        assert abs(got - r["value"]) <= r["tol"], r["label"]
+    bl = 2 * np.pi / sysm.aL
+    OUT.write_k_data(str(tmp_path / "Si_k.data"), kAc0, bl)
+    OUT.write_eigen_data(str(tmp_path / "Si_eigen.data"), np.sort(esp, axis=1), sysm.occ, sysm.NK)
+    _check_table(suite["001_bulk_gs"], str(tmp_path))
 
 
 @pytest.mark.parametrize("precision", ["c128", "c64"])
-def test_rt_current_and_energy_match_002(ground_state, precision):
+def test_rt_current_and_energy_match_002(ground_state, precision, tmp_path):
     from salmon_b200.rt import GpuSystem
     suite, sysm, kAc0, vpsl, esp, hist, zu = ground_state
     inp = suite["inputs"]
@@ -76,16 +84,12 @@ def test_rt_current_and_energy_match_002(ground_state, precision):
     with GpuSystem(sysm, precision) as g:
         g.set_state(zu)
         javt, energies = drive.rt_propagate(g, sysm, kAc0, vpsl, Ac, dt, nt + 1, energy_every=1, scf=True)
-    eall0 = energies[0]
-    for r in suite["002_bulk_rt"]:
-        it = r["row"]
-        if r["file"] == "Si_rt.data" and r["col"] == 15:
-            got = javt[it, 2]
-        elif r["file"] == "Si_rt_energy.data" and r["col"] == 2:
-            it = r["row"] * 10                                   # one row every nstep_energy_calc = 10 steps
-            e_tot = -(Ac[it + 2] - Ac[it]) / (2 * dt)
-            got = energies[it + 1] + sysm.aLxyz * float(e_tot @ e_tot) / (8 * np.pi) - eall0
-        else:
-            continue
-        print(f"{precision} {r['label']}: {got:+.6e} (ref {r['value']:+.4e}, tol {r['tol']:.0e})")
-        assert abs(got - r["value"]) <= r["tol"], (precision, r["label"], got)
+    # the rows as control_sc.f90 writes them: A and E = -dA/dt at step iter (transverse
+    # geometry: total = external), J after step iter-1, and Eall_t(iter) = the energy
+    # after step iter plus the field energy aLxyz |E|^2 / (8 pi)
+    E = OUT.fields_from_Ac(Ac, dt)
+    A = Ac[1:]
+    eall_t = {it: energies[it + 1] + sysm.aLxyz * float(E[it] @ E[it]) / (8 * np.pi) for it in range(nt + 1)}
+    OUT.write_rt_data(str(tmp_path / "Si_rt.data"), dt, A, E, A, E, javt, nt)
+    OUT.write_rt_energy_data(str(tmp_path / "Si_rt_energy.data"), dt, eall_t, energies[0], nt)
+    _check_table(suite["002_bulk_rt"], str(tmp_path), tag=precision + " ")
