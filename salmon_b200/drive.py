@@ -138,17 +138,19 @@ def band_energy(g, sysm, kAc, vloc):
     return ek + en + float(np.dot(vloc, rho)) * sysm.Hxyz
 
 
-def total_energy(g, sysm, kAc, vpsl):
-    """Ekin + Enl + sum Vpsl rho Hxyz + Eh + Exc of the resident orbitals (FP64;
-    the ion-ion term is a constant and left out); also rebuilds Vloc from their
-    density, as the reference's step does."""
+def total_energy(g, sysm, kAc, vpsl, eion: float = 0.0):
+    """Ekin + Enl + sum Vpsl rho Hxyz + Eh + Exc + eion of the resident orbitals
+    (FP64; eion is the ion-ion energy, a constant for fixed ions:
+    pseudo.ewald_energy); also rebuilds Vloc from their density, as the
+    reference's step does."""
     ek, en = g.energy_terms(kAc)
     rho = g.psi_rho_RT()
     eh, exc = g.update_vloc(rho)
-    return ek + en + float(np.dot(vpsl, rho)) * sysm.Hxyz + eh + exc
+    return ek + en + float(np.dot(vpsl, rho)) * sysm.Hxyz + eh + exc + eion
 
 
-def rt_propagate(g, sysm, kAc0, vloc, Ac, dt: float, Nt: int, energy_every: int = 0, scf: bool = False):
+def rt_propagate(g, sysm, kAc0, vloc, Ac, dt: float, Nt: int, energy_every: int = 0, scf: bool = False,
+                 eion: float = 0.0):
     """Nt middle-point Taylor steps of the resident orbitals; returns
     (javt (Nt+1,3) with javt[0] the current before the first step,
      energies {step: energy} every `energy_every` steps).
@@ -161,7 +163,7 @@ def rt_propagate(g, sysm, kAc0, vloc, Ac, dt: float, Nt: int, energy_every: int 
         g.update_vloc()
     else:
         g.set_vloc(vloc)
-    energy = (lambda k: total_energy(g, sysm, k, vloc)) if scf else (lambda k: band_energy(g, sysm, k, vloc))
+    energy = (lambda k: total_energy(g, sysm, k, vloc, eion)) if scf else (lambda k: band_energy(g, sysm, k, vloc))
     javt = np.zeros((Nt + 1, 3))
     javt[0] = g.current_RT(kAc0 + Ac[1][:, None])
     energies = {}

@@ -297,3 +297,38 @@ def from_npz(path: str, lloc: int, lmax_ps: int = -1) -> RadialPP:
     d = np.load(path)
     return from_tables(int(d["mr"]), float(d["step"]), int(d["mlps"]), float(d["zps"]), d["rrc"], d["vpp"],
                        d["upp"], lloc, lmax_ps)
+
+
+def ewald_energy(Rion, zps, aL, grid, n_ewald: int = 4, a_ewald: float = 0.5):
+    """Ion-ion energy by the Ewald sum of Total_Energy_omp (common/total_energy.f90:
+    58-108) with the defaults newald = 4, aewald = 0.5 (io/inputoutput.f90:786-787):
+    real-space images |n| <= n_ewald, the reciprocal sum over the grid's G set
+    (G != 0) with rho_ion(G) = sum_a Z_a e^{-iG.R_a} / |cell|, and the
+    self and neutralising-background terms.  zps: charge per atom."""
+    from math import erfc, pi, sqrt
+    Rion = np.asarray(Rion, dtype=np.float64)
+    z = np.broadcast_to(np.asarray(zps, dtype=np.float64), (Rion.shape[0],))
+    aL = np.asarray(aL, dtype=np.float64)
+    alxyz = float(aL[0] * aL[1] * aL[2])
+    e_real = 0.0
+    rng_ = range(-n_ewald, n_ewald + 1)
+    for ia in range(Rion.shape[0]):
+        for ix in rng_:
+            for iy in rng_:
+                for iz in rng_:
+                    shift = np.array([ix, iy, iz]) * aL
+                    for ib in range(Rion.shape[0]):
+                        if ix == 0 and iy == 0 and iz == 0 and ia == ib:
+                            continue
+                        rab = Rion[ia] - shift - Rion[ib]
+                        r = sqrt(float(rab @ rab))
+                        e_real += 0.5 * z[ia] * z[ib] * erfc(sqrt(a_ewald) * r) / r
+    gx, gy, gz, m0 = g_vectors(*grid, aL)
+    g2 = gx * gx + gy * gy + gz * gz
+    rho = np.zeros(g2.size, np.complex128)
+    for a in range(Rion.shape[0]):
+        rho += z[a] * np.exp(-1j * (gx * Rion[a, 0] + gy * Rion[a, 1] + gz * Rion[a, 2])) / alxyz
+    nz = np.arange(g2.size) != m0
+    e_g = float(np.sum(alxyz * (4 * pi / g2[nz]) * np.abs(rho[nz]) ** 2 * np.exp(-g2[nz] / (4 * a_ewald)) * 0.5))
+    e_self = -pi * float(z.sum()) ** 2 / (2 * a_ewald * alxyz) - sqrt(a_ewald / pi) * float((z * z).sum())
+    return e_real + e_g + e_self

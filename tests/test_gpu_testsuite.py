@@ -42,8 +42,8 @@ def ground_state(cuda_lib):
         g.gs_set_state(zu0)
         esp, hist = drive.gs_scf(g, sysm, kAc0, vpsl, nscf=inp["nscf"], ncg=inp["ncg"],
                                  threshold=inp["threshold"])
-        zu = g.get_state()
-    return suite, sysm, kAc0, vpsl, esp, hist, zu
+        zu_gs = g.gs_get_state()
+    return suite, sysm, kAc0, vpsl, esp, hist, zu_gs
 
 
 def _check_table(table, folder, tag=""):
@@ -74,8 +74,16 @@ def test_gs_eigenvalues_match_001(ground_state, tmp_path):
 
 @pytest.mark.parametrize("precision", ["c128", "c64"])
 def test_rt_current_and_energy_match_002(ground_state, precision, tmp_path):
+    """002_bulk_rt starts from the orbital files 001 wrote: the ground state goes
+    through gs_wfn_k/ (SALMON's unformatted layout) and is read back."""
+    from salmon_b200 import wfn_io
     from salmon_b200.rt import GpuSystem
-    suite, sysm, kAc0, vpsl, esp, hist, zu = ground_state
+    suite, sysm, kAc0, vpsl, esp, hist, zu_gs = ground_state
+    wfn_io.write_gs_wfn_k(str(tmp_path), zu_gs, sysm.occ)
+    zu_read, occ = wfn_io.read_gs_wfn_k(str(tmp_path), sysm.NK, sysm.NB, sysm.NL)
+    assert np.array_equal(occ, sysm.occ)
+    zu = np.ascontiguousarray(zu_read[:, :sysm.NBoccmax])   # zu_t = zu_GS(:,1:NBoccmax,:) (io_gs_wfn_k.f90:67)
+    eion = P.ewald_energy(sysm.Rion, sysm.extra["zps"], sysm.aL, (sysm.NLx, sysm.NLy, sysm.NLz))
     inp = suite["inputs"]
     dt, nt = inp["dt"], inp["nt"]
     # one step past nt: the energy row of step it is taken after that step (control_sc.f90:203-231)
@@ -83,7 +91,8 @@ def test_rt_current_and_energy_match_002(ground_state, precision, tmp_path):
                        omega=inp["omega1"], pulse_tw=inp["pulse_tw1"])
     with GpuSystem(sysm, precision) as g:
         g.set_state(zu)
-        javt, energies = drive.rt_propagate(g, sysm, kAc0, vpsl, Ac, dt, nt + 1, energy_every=1, scf=True)
+        javt, energies = drive.rt_propagate(g, sysm, kAc0, vpsl, Ac, dt, nt + 1, energy_every=1, scf=True,
+                                            eion=eion)
     # the rows as control_sc.f90 writes them: A and E = -dA/dt at step iter (transverse
     # geometry: total = external), J after step iter-1, and Eall_t(iter) = the energy
     # after step iter plus the field energy aLxyz |E|^2 / (8 pi)

@@ -144,3 +144,40 @@ def test_pulse_matches_002():
         else:
             continue
         assert abs(got - r["value"]) <= r["tol"], (r["label"], got)
+
+
+def test_ewald_energy_converges_and_is_independent_of_the_split():
+    """With a G set large enough (24^3) the Ewald sum does not depend on the
+    splitting parameter; diamond Si at a = 10.26 bohr gives about -8.40 Ry per atom.
+    On the 8^3 grid's G set the reciprocal sum is truncated, as in the reference."""
+    aL = np.array([10.26] * 3)
+    R = S.DIAMOND_RED * aL
+    e3 = P.ewald_energy(R, 4.0, aL, (24, 24, 24), a_ewald=0.3)
+    e5 = P.ewald_energy(R, 4.0, aL, (24, 24, 24), a_ewald=0.5)
+    assert abs(e3 - e5) < 1e-9 * abs(e5)
+    assert -8.45 < 2 * e5 / 8 < -8.35
+    assert abs(P.ewald_energy(R, 4.0, aL, (8, 8, 8)) - e5) > 0.1
+
+
+def test_gs_wfn_files_round_trip_and_layout(tmp_path):
+    from salmon_b200 import wfn_io
+    rng = np.random.default_rng(5)
+    NK, NB, NL = 3, 4, 10
+    zu = rng.standard_normal((NK, NB, NL)) + 1j * rng.standard_normal((NK, NB, NL))
+    occ = rng.uniform(0, 1, (NK, NB))
+    wfn_io.write_gs_wfn_k(str(tmp_path), zu, occ)
+    z2, o2 = wfn_io.read_gs_wfn_k(str(tmp_path), NK, NB, NL)
+    assert np.array_equal(z2, zu) and np.array_equal(o2, occ)
+    raw = (tmp_path / "gs_wfn_k" / "wfn_gs_k0000002.wfn").read_bytes()
+    n = NB * NL * 16
+    assert len(raw) == n + 8
+    assert int.from_bytes(raw[:4], "little") == n and int.from_bytes(raw[-4:], "little") == n
+    # column-major zu_GS(NL, NB): the first NL values are band 1 of k-point 2
+    first = np.frombuffer(raw[4:4 + 16 * NL], dtype="<c16")
+    assert np.array_equal(first, zu[1, 0])
+    occ_raw = (tmp_path / "gs_wfn_k" / "occupation").read_bytes()
+    assert np.array_equal(np.frombuffer(occ_raw[4:-4], dtype="<f8")[:NB], occ[0])   # occ(1:NB, 1)
+    # a damaged record is refused
+    (tmp_path / "gs_wfn_k" / "wfn_gs_k0000003.wfn").write_bytes(raw[:-2])
+    with pytest.raises(ValueError):
+        wfn_io.read_gs_wfn_k(str(tmp_path), NK, NB, NL)
