@@ -180,13 +180,14 @@ size_t pass_smem_bytes(int prec, int NLy, int NLz, int maxpts, bool with_w, int 
 // global loads off each march step.
 //
 // GY, GZ (non-zero: the plane shape NLy x NLz at compile time, complex(4), two-point
-// table form without y-blocks): the ring then has one slot per unrolled phase (NR = 9),
-// so every ring, table and neighbour offset is a compile-time constant and the
-// per-step address arithmetic drops to a few adds.
-template <typename R, int RZ, int MODE, bool YB, bool TB, int GY = 0, int GZ = 0>
+// table form; GB: the rows of a y-block, with YB): the ring then has one slot per
+// unrolled phase (NR = 9), so every ring, table and neighbour offset is a
+// compile-time constant and the per-step address arithmetic drops to a few adds.
+template <typename R, int RZ, int MODE, bool YB, bool TB, int GY = 0, int GZ = 0, int GB = 0>
 __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
   static_assert(!TB || RZ == 2, "table staging copies the two points' entries as one run");
-  static_assert(GZ == 0 || (std::is_same<R, float>::value && TB && !YB), "fixed shapes: complex(4) table form");
+  static_assert(GZ == 0 || (std::is_same<R, float>::value && TB && (YB == (GB > 0))),
+                "fixed shapes: complex(4) table form; y-block rows with y-blocks only");
   using T = C2<R>;
   constexpr bool FIXED = GZ > 0;
   constexpr int NR = FIXED ? 9 : PassGeom<R>::NR;
@@ -194,12 +195,13 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
   const int NLy = FIXED ? GY : a.NLy, NLz = FIXED ? GZ : a.NLz, NYZ = NLy * NLz;
   const bool with_w = a.W != nullptr;
   const bool do_export = a.S != nullptr;
-  const int nyblk = YB ? a.nyblk : 1;
-  const int RYZ = YB ? (a.NYB + 8) * NLz : NYZ;  // ring plane size
+  const int NYBc = YB ? (FIXED ? GB : a.NYB) : NLy;  // rows of a y-block
+  const int nyblk = YB ? (FIXED ? (GY + GB - 1) / GB : a.nyblk) : 1;
+  const int RYZ = YB ? (NYBc + 8) * NLz : NYZ;  // ring plane size
   T* ring = reinterpret_cast<T*>(smem_raw);
   T* wring = ring + (size_t)NR * RYZ;  // [NR][maxpts] W chunks of the ring's planes
   constexpr bool tab = TB;
-  const int TYZ = YB ? a.NYB * NLz : NYZ;  // table plane size (owned rows)
+  const int TYZ = YB ? NYBc * NLz : NYZ;  // table plane size (owned rows)
   R* vtab = reinterpret_cast<R*>(wring + (with_w ? (size_t)NR * a.maxpts : 0));  // [NR][TYZ] (tab)
   short* lqtab = reinterpret_cast<short*>(vtab + (tab ? (size_t)NR * TYZ : 0));    // [NR][TYZ] (tab)
   // sp_off[0..NLx] (or sp_blk in the YB form)
@@ -213,7 +215,7 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
 
   const int b = YB ? blockIdx.x / nyblk : blockIdx.x;
   const int yb = YB ? blockIdx.x - b * nyblk : 0;
-  const int y0 = YB ? yb * a.NYB : 0;
+  const int y0 = YB ? yb * NYBc : 0;
   const int o = a.o_beg + b;
   const int kl = o / a.NBocc;
   const double kxd = a.kAc[3 * kl], kyd = a.kAc[3 * kl + 1], kzd = a.kAc[3 * kl + 2];
@@ -233,7 +235,7 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
   const int NZG = NLz / RZ;
   const int t = threadIdx.x;
   const int bd = blockDim.x;
-  const int ny_own = YB ? min(a.NYB, NLy - y0) : NLy;
+  const int ny_own = YB ? min(NYBc, NLy - y0) : NLy;
   const bool act = t < ny_own * NZG;
   const int yl = act ? t / NZG : 0;  // row in the block
   const int y = y0 + yl;             // row in the plane
@@ -259,7 +261,7 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
       if (jn < nplanes) {  // the block's rows and the halo rows, periodic in y
         T* dst = ring + (size_t)sl * RYZ;
         const T* src = inb + (size_t)p * NYZ;
-        for (int idx = t; idx < (a.NYB + 8) * NZG; idx += bd) {
+        for (int idx = t; idx < (NYBc + 8) * NZG; idx += bd) {
           const int r = idx / NZG, zz = (idx - r * NZG) * RZ;
           int gy = y0 - 4 + r;
           gy += gy < 0 ? NLy : 0;
@@ -510,9 +512,11 @@ static bool pass_tables(const System& s, int RZ) {
   return true;
 }
 
-// plane shapes with a compile-time form (complex(4), table form, no y-blocks):
-// the 16^3, 20^3 and 32^3 grids and the 16x16x32 supercell
-static int fixed_shape(int NLy, int NLz) {
+// plane shapes with a compile-time form (complex(4), table form): the 16^3, 20^3
+// and 32^3 grids and the 16x16x32 supercell without y-blocks, 48x48 planes in
+// three y-blocks of 16 rows (the 48^3 grid)
+static int fixed_shape(int NLy, int NLz, int nyblk, int NYB) {
+  if (nyblk > 1) return (NLy == 48 && NLz == 48 && nyblk == 3 && NYB == 16) ? 5 : 0;
   if (NLy == 32 && NLz == 32) return 1;
   if (NLy == 16 && NLz == 16) return 2;
   if (NLy == 16 && NLz == 32) return 3;
@@ -532,6 +536,7 @@ static void (*pass_kernel(bool yb, bool tb, int shape))(const PassArgs<R>) {
         default: break;
       }
     }
+    if (tb && yb && shape == 5) return k_hpsi_pass<R, RZ, MODE, true, true, 48, 48, 16>;
   }
   if constexpr (RZ == 2) {
     if (tb) return yb ? k_hpsi_pass<R, RZ, MODE, true, true> : k_hpsi_pass<R, RZ, MODE, false, true>;
@@ -543,9 +548,10 @@ static void (*pass_kernel(bool yb, bool tb, int shape))(const PassArgs<R>) {
 // its 9-plane ring must fit in shared memory
 template <typename R, int RZ>
 static int pass_shape(const System& s, bool tb) {
-  if (!std::is_same<R, float>::value || RZ != 2 || !tb || s.nyblk > 1 || !s.pass_fixed) return 0;
-  const int sh = fixed_shape(s.NLy, s.NLz);
-  if (sh && pass_smem_bytes(SGPU_PREC_C64, s.NLy, s.NLz, s.maxpts, true, s.NLx, 1, s.NLy, true, 9) > 227 * 1024)
+  if (!std::is_same<R, float>::value || RZ != 2 || !tb || !s.pass_fixed) return 0;
+  const int sh = fixed_shape(s.NLy, s.NLz, s.nyblk, s.NYB);
+  const int nyb = s.nyblk > 1 ? s.NYB : s.NLy;
+  if (sh && pass_smem_bytes(SGPU_PREC_C64, s.NLy, s.NLz, s.maxpts, true, s.NLx, s.nyblk, nyb, true, 9) > 227 * 1024)
     return 0;
   return sh;
 }
