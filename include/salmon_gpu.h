@@ -282,9 +282,11 @@ enum {
   SGPU_PARAM_KB_KERNEL = 5,   /* KB term of H psi: 1 band-group tile kernel (32 bands of a k-point per
                                  CTA, pipelined gathers), 2 band-quad kernel (UVPSI_SPLIT warps per
                                  4 bands), 0 the tile kernel when its grid has >= 2 CTAs per SM       */
-  SGPU_PARAM_PASS_FIXED = 6   /* stencil pass, complex(4): 1 uses the compile-time plane shapes
-                                 (16x16, 16x32, 20x20, 32x32 planes: 9-plane ring, constant offsets)
-                                 where they fit, 0 the generic kernel                                 */
+  SGPU_PARAM_PASS_FIXED = 6,  /* stencil pass, complex(4): 1 uses the compile-time plane shapes
+                                 (16x16, 16x32, 20x20, 32x32 planes, 48x48 in three y-blocks: 9-plane
+                                 ring, constant offsets) where they fit, 0 the generic kernel         */
+  SGPU_PARAM_CUR_FIXED = 7    /* current stencil, 32x32 planes: 1 splits each plane over four CTAs,
+                                 2 over two, 0 the generic one-CTA x-march                           */
 };
 
 /* CG preconditioners.  PLAIN is the reference's CG_ompk.  TPA multiplies the

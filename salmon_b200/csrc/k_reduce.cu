@@ -96,10 +96,15 @@ struct Nab12 {
   double v[12];  // nabx(1:4), naby(1:4), nabz(1:4): kernel parameters, read from the parameter bank
 };
 
-template <typename R, int NT, int P, int D>
-__global__ void __launch_bounds__(NT, 1) k_current_march(const C2<R>* __restrict__ zu, int NLx, int NLy, int NLz,
-                                                       const Nab12 nab, double* __restrict__ out) {
+//
+// GY, GZ (non-zero): the plane shape at compile time, so the neighbour offsets are
+// shifts and masks the compiler recomputes instead of holding them in registers;
+// MB: CTAs per SM the register budget is cut for.
+template <typename R, int NT, int P, int D, int GY = 0, int GZ = 0, int MB = 1>
+__global__ void __launch_bounds__(NT, MB) k_current_march(const C2<R>* __restrict__ zu, int NLx, int NLy_, int NLz_,
+                                                        const Nab12 nab, double* __restrict__ out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int NLy = GZ ? GY : NLy_, NLz = GZ ? GZ : NLz_;
   const int NYZ = NLy * NLz;
   double2* buf = reinterpret_cast<double2*>(smem_raw);  // [2][NYZ]
   __shared__ double sh[32 * 4];
@@ -189,6 +194,75 @@ __global__ void __launch_bounds__(NT, 1) k_current_march(const C2<R>* __restrict
     out[4 * (size_t)o + 2] = v[2];
     out[4 * (size_t)o + 3] = v[3];
   }
+}
+
+// The x-march with each GY x GZ plane split over NP CTAs of GY/NP rows (one
+// point per thread, (GY/NP)*GZ threads): a CTA stages its rows and the four rows
+// after them (the forward y-neighbours, read from L2 each step) in FP64 in
+// shared memory.  Small CTAs at few registers let several orbitals' marches
+// share an SM, so one CTA's barrier waits overlap another's arithmetic.
+// out[o][h][4], h = the part.
+template <typename R, int GY, int GZ, int NP>
+__global__ void __launch_bounds__(GY / NP * GZ) k_current_march_yh(const C2<R>* __restrict__ zu, int NLx,
+                                                                  const Nab12 nab, double* __restrict__ out) {
+  constexpr int NYH = GY / NP, NT = NYH * GZ, NYZ = GY * GZ, RB = (NYH + 4) * GZ;
+  static_assert(NT % 32 == 0 && NT <= 1024 && 4 * GZ <= NT, "one point per thread, halo loaded by the first rows");
+  __shared__ double2 buf[2][RB];
+  __shared__ double sh[32 * 4];
+  const int o = blockIdx.x / NP, h = blockIdx.x - (blockIdx.x / NP) * NP, t = threadIdx.x;
+  const C2<R>* E = zu + (size_t)o * NLx * NYZ;
+  const double* nb = nab.v;
+  const int yl = t / GZ, z = t - (t / GZ) * GZ;
+  const int own = (h * NYH + yl) * GZ + z;                           // in the plane
+  const int hrow = ((h + 1) * NYH + (t / GZ)) % GY;                   // halo row of threads t < 4 GZ
+  const int hsrc = hrow * GZ + z;
+  double2 q[5];
+#pragma unroll
+  for (int m = 0; m < 5; ++m) q[m] = to_d2(__ldg(E + (size_t)(m % NLx) * NYZ + own));
+  C2<R> nxt = __ldg(E + (size_t)(5 % NLx) * NYZ + own);
+  double v[4] = {0, 0, 0, 0};
+  for (int x = 0; x < NLx; ++x) {
+    double2* pl = buf[x & 1];
+    pl[t] = q[0];
+    if (t < 4 * GZ) pl[NT + t] = to_d2(__ldg(E + (size_t)x * NYZ + hsrc));
+    __syncthreads();
+    const double2 e = q[0];
+    v[0] += e.x * e.x + e.y * e.y;
+    double2 sx = make_double2(0, 0), sy = make_double2(0, 0), sz = make_double2(0, 0);
+#pragma unroll
+    for (int n = 1; n <= 4; ++n) {
+      const double2 ex = q[n];
+      const double2 ey = pl[(yl + n) * GZ + z];
+      const double2 ez = pl[yl * GZ + ((z + n) % GZ)];
+      sx.x += nb[n - 1] * ex.x; sx.y += nb[n - 1] * ex.y;
+      sy.x += nb[3 + n] * ey.x; sy.y += nb[3 + n] * ey.y;
+      sz.x += nb[7 + n] * ez.x; sz.y += nb[7 + n] * ez.y;
+    }
+    v[1] += e.x * sx.y - e.y * sx.x;
+    v[2] += e.x * sy.y - e.y * sy.x;
+    v[3] += e.x * sz.y - e.y * sz.x;
+    q[0] = q[1];
+    q[1] = q[2];
+    q[2] = q[3];
+    q[3] = q[4];
+    q[4] = to_d2(nxt);
+    nxt = __ldg(E + (size_t)((x + 6) % NLx) * NYZ + own);
+  }
+  block_sum<4>(v, sh);
+  if (t == 0) {
+    double* d = out + 4 * (size_t)blockIdx.x;
+    d[0] = v[0];
+    d[1] = v[1];
+    d[2] = v[2];
+    d[3] = v[3];
+  }
+}
+
+template <typename R, int GY, int GZ, int NP>
+static cudaError_t current_march_yh(System& s, const Nab12& nab, double* out) {
+  k_current_march_yh<R, GY, GZ, NP><<<NP * s.norb, GY / NP * GZ, 0, s.launch_stream()>>>((const C2<R>*)s.zu, s.NLx,
+                                                                                          nab, out);
+  return cudaGetLastError();
 }
 
 // Planes of more than 1024 points: one CTA per (orbital, x-plane), the
@@ -405,16 +479,16 @@ static size_t uvpsi_w_smem(int n, size_t e) { return (size_t)n * (8 * e + sizeof
 // and of launch_energy (part [norb][NLx][2], eo [norb][2], 25 coefficients)
 size_t current_red_elems(int norb, int NLx) { return (size_t)norb * NLx * 4 + 3 * (size_t)norb + 32; }
 
-template <typename R, int NT, int P, int D>
+template <typename R, int NT, int P, int D, int GY = 0, int GZ = 0, int MB = 1>
 static cudaError_t current_march(System& s, const Nab12& nab, double* out) {
   const size_t smem = 2 * (size_t)s.NLy * s.NLz * sizeof(double2);
   if (smem > 48 * 1024) {
-    const cudaError_t e =
-        cudaFuncSetAttribute(k_current_march<R, NT, P, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const cudaError_t e = cudaFuncSetAttribute(k_current_march<R, NT, P, D, GY, GZ, MB>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  k_current_march<R, NT, P, D><<<s.norb, NT, smem, s.launch_stream()>>>((const C2<R>*)s.zu, s.NLx, s.NLy, s.NLz, nab,
-                                                                        out);
+  k_current_march<R, NT, P, D, GY, GZ, MB><<<s.norb, NT, smem, s.launch_stream()>>>((const C2<R>*)s.zu, s.NLx, s.NLy,
+                                                                                    s.NLz, nab, out);
   return cudaGetLastError();
 }
 
@@ -427,6 +501,13 @@ template <typename R>
 static cudaError_t current_stencil(System& s, const Nab12& nab, const double* nab12, double* part, int& nx) {
   const int NYZ = s.NLy * s.NLz;
   nx = 1;
+  // 32x32 planes: four CTAs of 8 rows per orbital plane (value 2: two of 16 rows).
+  // sgpu_current at 32^3 x 2048 orbitals, complex(4): 0.80 ms, two parts 0.85 ms,
+  // the one-CTA x-march 0.95 ms (complex(8): 0.91 / 0.96 / 1.12 ms)
+  if (s.cur_fixed && s.NLy == 32 && s.NLz == 32) {
+    nx = s.cur_fixed == 2 ? 2 : 4;
+    return s.cur_fixed == 2 ? current_march_yh<R, 32, 32, 2>(s, nab, part) : current_march_yh<R, 32, 32, 4>(s, nab, part);
+  }
   if (NYZ <= 256) return current_march<R, 256, 1, 1>(s, nab, part);
   if (NYZ <= 512) return current_march<R, 512, 1, 1>(s, nab, part);
   if (NYZ <= 1024) return current_march<R, 1024, 1, 1>(s, nab, part);

@@ -927,6 +927,10 @@ extern "C" int sgpu_set_param(sgpu_handle h, int param, int value) {
       if (value < 0 || value > 2) return fail(SGPU_ERR_ARG, "sgpu_set_param: KB kernel must be 0, 1 or 2");
       s->kb_kernel = value;
       return 0;
+    case SGPU_PARAM_CUR_FIXED:
+      if (value < 0 || value > 2) return fail(SGPU_ERR_ARG, "sgpu_set_param: current fixed shape must be 0, 1 or 2");
+      s->cur_fixed = value;
+      return 0;
     case SGPU_PARAM_PASS_FIXED:
       if (value != 0 && value != 1) return fail(SGPU_ERR_ARG, "sgpu_set_param: pass fixed shapes must be 0 or 1");
       s->pass_fixed = value;
@@ -951,6 +955,7 @@ extern "C" int sgpu_get_param(sgpu_handle h, int param, int* value) {
     case SGPU_PARAM_PASS_TABLES: *value = h->pass_tab; return 0;
     case SGPU_PARAM_KB_KERNEL: *value = h->kb_kernel; return 0;
     case SGPU_PARAM_PASS_FIXED: *value = h->pass_fixed; return 0;
+    case SGPU_PARAM_CUR_FIXED: *value = h->cur_fixed; return 0;
     default: return fail(SGPU_ERR_ARG, "sgpu_get_param: unknown parameter");
   }
 }

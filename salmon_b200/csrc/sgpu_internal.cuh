@@ -192,6 +192,7 @@ struct System {
   int* sp_blk = nullptr;           // [NLx*(nyblk+1)] first sphere point of each (plane, y-block)
   int pass_tab = 1;                // stencil pass: Vloc/sphere-index tables through the ring (two-point form)
   int pass_fixed = 1;              // stencil pass: compile-time plane shapes with a 9-plane ring (complex(4))
+  int cur_fixed = 1;               // current stencil, 32x32 planes: 1 four CTAs per plane, 2 two, 0 one
   int nsm = 148;                   // SMs of the device
   mutable bool kb_smem_ok = false;  // the KB tile kernels' shared-memory limits are raised for this handle
   int um_split = 4;                // band-quad KB kernel: warps splitting the points of one tile (1, 2, 4, 8)
