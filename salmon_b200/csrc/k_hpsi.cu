@@ -444,7 +444,7 @@ static cudaError_t launch_kb_fused_split(const System& s, const void* in, int ld
 constexpr int KBT_WARPS = 8;               // band quads per CTA
 constexpr int KBT_KS = 2;                  // warps per band quad
 constexpr int KBT_BANDS = 4 * KBT_WARPS;   // bands per CTA
-constexpr int KBT_NS = 3;                  // pipeline stages
+constexpr int KBT_NS = 4;                  // pipeline stages
 template <typename R>
 struct KbtGeom {
   static constexpr bool F = std::is_same<R, float>::value;
@@ -532,12 +532,11 @@ __global__ void __launch_bounds__(32 * KBT_WARPS * KBT_KS) k_kb_tile(const C2<R>
   const int pa = n & 3, zpart = n >> 2;                    // A row n: projector n%4, Re (n<4) / Im
   const int bb = 4 * warp + (n >> 1), bpart = n & 1;       // B column n: band n/2 of the quad, Re/Im
   double c0 = 0.0, c1 = 0.0, e0 = 0.0, e1 = 0.0;
-  issue(0, true);
-  issue(1, true);
+  for (int c = 0; c < KBT_NS - 1; ++c) issue(c, true);
   for (int c = 0; c < nch; ++c) {
-    cp_async_wait<1>();  // this thread's copies of chunk c have landed
-    __syncthreads();     // ... everyone's; the stage of chunk c-1 is free
-    issue(c + 2, true);
+    cp_async_wait<KBT_NS - 2>();  // this thread's copies of chunk c have landed
+    __syncthreads();              // ... everyone's; the stage of chunk c-1 is free
+    issue(c + KBT_NS - 1, true);
     const int s = c % KBT_NS;
     const T* sb = Sb + (size_t)s * KBT_BANDS * SROW + bb * SROW;
     const double* za = reinterpret_cast<const double*>(Zb + (size_t)s * 4 * ZROW + pa * ZROW) + zpart;
@@ -582,12 +581,11 @@ __global__ void __launch_bounds__(32 * KBT_WARPS * KBT_KS) k_kb_tile(const C2<R>
   const int oc = o_lo + 4 * warp + p;       // the orbital of this lane's C elements
   const bool cvalid = oc < o_hi;
   T* Wb = W + (size_t)(cvalid ? oc - o_beg : 0) * nsp;
-  issue(0, false);
-  issue(1, false);
+  for (int c = 0; c < KBT_NS - 1; ++c) issue(c, false);
   for (int c = 0; c < nch; ++c) {
-    cp_async_wait<1>();
+    cp_async_wait<KBT_NS - 2>();
     __syncthreads();
-    issue(c + 2, false);
+    issue(c + KBT_NS - 1, false);
     const double2* zb = Zb + (size_t)(c % KBT_NS) * 4 * ZROW + p * ZROW;
 #pragma unroll
     for (int t8 = ks; t8 < CP / 8; t8 += KBT_KS) {
