@@ -366,11 +366,18 @@ def precond_bench(max_outer=60):
                         f"{max_outer} outer iterations)"}
 
 
+def bench_config(args, sysm, norb, world):
+    """The `config` of both arms' JSON lines (the same workload description)."""
+    return {"workload": f"hpsi/Taylor microbench {args.grid}^3, {sysm.NK} k x {sysm.NBoccmax} bands per GPU",
+            "grid": args.grid, "nk": sysm.NK, "nb": sysm.NBoccmax, "norb_per_gpu": norb,
+            "l2": "inputs larger than L2 at every pass (no flush)", "parallelism": f"k-blocks x{world}"}
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    sysm, kAc, vloc, zu = make_workload(args, 0)
+    sysm, kAc, vloc, zu = make_workload(args, 0, world)
     from oracle import oracle as O
     if not O.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (SALMON AVX stencil build) missing"}))
@@ -386,8 +393,7 @@ def run_reference(args):
     out = {"metric": METRIC, "value": v, "unit": "orbital-updates/s", "n_gpus": 0, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": 1000.0 * norb / v, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-           "config": {"workload": f"hpsi/Taylor microbench {args.grid}^3, {sysm.NK} k x {sysm.NBoccmax} bands",
-                      "grid": args.grid, "nk": sysm.NK, "nb": sysm.NBoccmax},
+           "config": bench_config(args, sysm, norb, world),
            "impl": "reference", "cpu_baseline": {k: vals[-1][k] for k in ("kind", "cores", "sample")} | {"value": v, "unit": "orbital-updates/s"},
            "e2e": {"value": v, "unit": "orbital-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
@@ -533,9 +539,7 @@ def main():
             "metric": METRIC, "value": h["value"], "unit": "orbital-updates/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": h["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c64 orbitals (FP32 stencil), FP64 reductions", "data": "synthetic",
-            "config": {"workload": f"hpsi/Taylor microbench {args.grid}^3, {sysm.NK} k x {sysm.NBoccmax} bands per GPU",
-                       "grid": args.grid, "nk": sysm.NK, "nb": sysm.NBoccmax, "norb_per_gpu": norb,
-                       "l2": "inputs larger than L2 at every pass (no flush)", "parallelism": f"k-blocks x{world}"},
+            "config": bench_config(args, sysm, norb, world),
             "fp64_path": {"value": res["c128"]["value"], "ms_per_step": res["c128"]["ms_per_step"],
                           "e2e": res["c128"]["e2e"], "stencil_pass_ms": res["c128"]["t_pass_ms"],
                           "stencil_pass_gbs": res["c128"]["achieved_gbs"]},
