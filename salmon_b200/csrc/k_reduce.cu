@@ -332,92 +332,119 @@ __global__ void __launch_bounds__(256, 2) k_current_plane(const C2<R>* __restric
 // psi(J(j)) is read from src[o*ld + idx[j]]: the compact sphere values S with
 // the sphere-point map qmap when they are current, else the orbitals with the
 // grid index idx_proj.
-// One CTA per (projector item, k-point) serves every band of that k-point.
-// Work units are (band, projector) pairs, band-major, one per warp and round;
-// the round's band values at the item's points are gathered into shared memory
-// by all threads (eight loads in flight per thread), the projector rows and
-// positions are read through L1.  Lanes split the points; lane sums are combined
-// by shuffles (fixed order).
+// One CTA per (projector item, k-point) and group of up to 32 bands of that
+// k-point computes the complex product C[band][p,w] = sum_j psi_b(j) B_j[p,w],
+// B_j[p,w] = conj(zproj_p(j)) r_w(j), in chunks of UVW_CH points: the chunk's B
+// (16 entries per point) and the bands' values at its points are staged in shared
+// memory (band rows padded by one element against bank conflicts); thread (tile,
+// part) accumulates a tile of 4 bands x the 4 weights of one projector over every
+// eighth point in FP64, and the eight parts are added in a fixed order.
+constexpr int UVW_CH = 128;
+template <typename R> struct UvwGeom {
+  static constexpr int SROW = UVW_CH + 1;  // padded band row
+  static constexpr size_t smem =
+      sizeof(C2<R>) * 32 * SROW + sizeof(double2) * 16 * UVW_CH + sizeof(int) * UVW_CH;
+};
+
 template <typename R>
 __global__ void __launch_bounds__(256, 2) k_uvpsi_w(const C2<R>* __restrict__ src, int ld, int NBocc,
-                                                  const double2* __restrict__ zproj, int Nlma, int Nps,
-                                                  const int* __restrict__ idx, const int* __restrict__ atom_off,
-                                                  const double* __restrict__ rpos, const int4* __restrict__ items,
-                                                  const int* __restrict__ lma_list, int chunk,
-                                                  double2* __restrict__ Uw) {
+                                                     const double2* __restrict__ zproj, int Nlma, int Nps,
+                                                     const int* __restrict__ idx, const int* __restrict__ atom_off,
+                                                     const double* __restrict__ rpos, const int4* __restrict__ items,
+                                                     const int* __restrict__ lma_list, double2* __restrict__ Uw) {
+  constexpr int CH = UVW_CH, SROW = UvwGeom<R>::SROW;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  C2<R>* ps = reinterpret_cast<C2<R>*>(smem_raw);                // [nw][chunk] band values
-  int* is = reinterpret_cast<int*>(ps + (size_t)nw * chunk);     // [chunk]
+  C2<R>* ps = reinterpret_cast<C2<R>*>(smem_raw);                          // [32][SROW] band values
+  double2* Bs = reinterpret_cast<double2*>(ps + 32 * SROW);                 // [CH][16] weighted rows
+  int* is = reinterpret_cast<int*>(Bs + 16 * CH);                          // [CH] gather index
+  double2* red = reinterpret_cast<double2*>(smem_raw);                     // [8][32][16] after the sums
+  const int t = threadIdx.x, lane = t & 31, part = t >> 5;
+  const int bg = lane & 7, pg = lane >> 3;  // bands 4bg..4bg+3, projector pg (its 4 weights)
   const int4 item = items[blockIdx.x];
-  const int kl = blockIdx.y;
+  const int kl = blockIdx.y, b0 = blockIdx.z * 32;
   const int a = item.x, l0 = item.y, np = item.z;
   const int p0 = atom_off[a], mps = atom_off[a + 1] - p0;
-  const int bpr = nw / np;                      // bands per round
-  const int nrounds = (NBocc + bpr - 1) / bpr;
-  const int wb = warp / np, wp = warp - wb * np;  // this warp's band slot and projector
-  const bool wact = wb < bpr;
-  const int ilma = lma_list[l0 + (wact ? wp : 0)];
-  const double2* zrow = zproj + ((size_t)kl * Nlma + ilma) * Nps;
-  for (int rd = 0; rd < nrounds; ++rd) {
-    const int b = rd * bpr + wb;
-    const int nbr = min(bpr, NBocc - rd * bpr);
-    double2 acc[4];
+  const int nbr = min(32, NBocc - b0);
+  if (nbr <= 0) return;  // whole CTA leaves together
+  double2 acc[4][4];
 #pragma unroll
-    for (int w = 0; w < 4; ++w) acc[w] = make_double2(0, 0);
-    for (int c0 = 0; c0 < mps; c0 += chunk) {
-      const int len = min(chunk, mps - c0);
-      __syncthreads();  // ps / is of the previous chunk or round are no longer read
-      for (int j = threadIdx.x; j < len; j += blockDim.x) is[j] = idx[p0 + c0 + j];
-      __syncthreads();
-      const int tot = nbr * len;
-      for (int q0 = threadIdx.x; q0 < tot; q0 += 8 * blockDim.x) {
-        C2<R> vals[8];
-        int slot[8];
+  for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
-          const int q = q0 + u * blockDim.x;
-          slot[u] = -1;
-          if (q < tot) {
-            const int bb = q / len, j = q - bb * len;
-            slot[u] = bb * chunk + j;
-            vals[u] = __ldg(src + (size_t)(kl * NBocc + rd * bpr + bb) * ld + is[j]);
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < 8; ++u)
-          if (slot[u] >= 0) ps[slot[u]] = vals[u];
+    for (int w = 0; w < 4; ++w) acc[i][w] = make_double2(0.0, 0.0);
+  for (int c0 = 0; c0 < mps; c0 += CH) {
+    const int len = min(CH, mps - c0);
+    __syncthreads();  // the previous chunk is no longer read
+    for (int q = t; q < 4 * CH; q += 256) {  // B of point j, projector p
+      const int p = q / CH, j = q - p * CH;
+      double2 z = make_double2(0.0, 0.0);
+      double r1 = 0.0, r2 = 0.0, r3 = 0.0;
+      if (j < len && p < np) {
+        z = zproj[((size_t)kl * Nlma + lma_list[l0 + p]) * Nps + c0 + j];
+        const double* r = rpos + 3 * (size_t)(p0 + c0 + j);
+        r1 = r[0]; r2 = r[1]; r3 = r[2];
       }
-      __syncthreads();
-      if (wact && b < NBocc) {
-        const C2<R>* pw = ps + (size_t)wb * chunk;
-        for (int j = lane; j < len; j += 32) {
-          const double2 e = to_d2(pw[j]);
-          const double2 z = __ldg(zrow + c0 + j);
-          const double* r = rpos + 3 * (size_t)(p0 + c0 + j);
-          const double rw[4] = {1.0, __ldg(r), __ldg(r + 1), __ldg(r + 2)};
-          // conj(z) * e
-          const double2 ze = make_double2(z.x * e.x + z.y * e.y, z.x * e.y - z.y * e.x);
+      const double2 cz = make_double2(z.x, -z.y);  // conj(zproj)
+      double2* bd = Bs + j * 16 + 4 * p;
+      bd[0] = cz;
+      bd[1] = make_double2(cz.x * r1, cz.y * r1);
+      bd[2] = make_double2(cz.x * r2, cz.y * r2);
+      bd[3] = make_double2(cz.x * r3, cz.y * r3);
+      if (p == 0 && j < len) is[j] = idx[p0 + c0 + j];
+    }
+    __syncthreads();
+    const int tot = 32 * len;
+    for (int q0 = t; q0 < tot; q0 += 8 * 256) {
+      C2<R> vals[8];
+      int slot[8];
 #pragma unroll
-          for (int w = 0; w < 4; ++w) {
-            acc[w].x += rw[w] * ze.x;
-            acc[w].y += rw[w] * ze.y;
-          }
+      for (int u = 0; u < 8; ++u) {
+        const int q = q0 + u * 256;
+        slot[u] = -1;
+        if (q < tot) {
+          const int bb = q / len, j = q - bb * len;
+          slot[u] = bb * SROW + j;
+          vals[u] = bb < nbr ? __ldg(src + (size_t)(kl * NBocc + b0 + bb) * ld + is[j]) : C2<R>{};
         }
       }
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (slot[u] >= 0) ps[slot[u]] = vals[u];
     }
-    if (wact && b < NBocc) {
+    __syncthreads();
+    for (int j = part; j < len; j += 8) {
+      double2 e[4], bw[4];
 #pragma unroll
-      for (int w = 0; w < 4; ++w)
+      for (int i = 0; i < 4; ++i) e[i] = to_d2(ps[(4 * bg + i) * SROW + j]);
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-          acc[w].x += __shfl_xor_sync(0xffffffffu, acc[w].x, off);
-          acc[w].y += __shfl_xor_sync(0xffffffffu, acc[w].y, off);
+      for (int w = 0; w < 4; ++w) bw[w] = Bs[j * 16 + 4 * pg + w];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {  // acc += e * B
+          acc[i][w].x += e[i].x * bw[w].x - e[i].y * bw[w].y;
+          acc[i][w].y += e[i].x * bw[w].y + e[i].y * bw[w].x;
         }
-      if (lane == 0)
-#pragma unroll
-        for (int w = 0; w < 4; ++w) Uw[((size_t)(kl * NBocc + b) * Nlma + ilma) * 4 + w] = acc[w];
     }
+  }
+  __syncthreads();  // the staging buffers are reused for the part sums
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int w = 0; w < 4; ++w) red[(part * 32 + lane) * 16 + 4 * i + w] = acc[i][w];
+  __syncthreads();
+  for (int q = t; q < 32 * 16; q += 256) {  // (tile, entry): sum the 8 parts in order
+    const int tile = q >> 4, k = q & 15;
+    double2 sum = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int pp = 0; pp < 8; ++pp) {
+      const double2 v = red[(pp * 32 + tile) * 16 + k];
+      sum.x += v.x;
+      sum.y += v.y;
+    }
+    const int tb = tile & 7, tp = tile >> 3, i = k >> 2, w = k & 3;
+    const int b = 4 * tb + i;
+    if (tp < np && b < nbr)
+      Uw[((size_t)(kl * NBocc + b0 + b) * Nlma + lma_list[l0 + tp]) * 4 + w] = sum;
   }
 }
 
@@ -472,8 +499,6 @@ __global__ void k_current_sum(const double* __restrict__ jo, int norb, double* _
   }
 }
 
-// shared memory of k_uvpsi_w for a chunk of n points and 8 warps' band values of e bytes each
-static size_t uvpsi_w_smem(int n, size_t e) { return (size_t)n * (8 * e + sizeof(int)); }
 
 // scratch of launch_current (part [norb][NLx][4], jo [norb][3], 12 coefficients)
 // and of launch_energy (part [norb][NLx][2], eo [norb][2], 25 coefficients)
@@ -534,16 +559,14 @@ cudaError_t launch_current(System& s, double* jav_dev) {
                               : current_stencil<double>(s, nab, nab12, part, nx);
   if (e != cudaSuccess) return e;
   if (s.Nlma && s.nitems) {
-    // chunks of at most 1024 (complex(4)) or 512 (complex(8)) points: 66-68 KB of shared memory per CTA
-    const int chunk = std::min(std::max(s.max_mps, 1), s.prec == SGPU_PREC_C64 ? 1024 : 512);
-    const size_t smem = uvpsi_w_smem(chunk, s.prec == SGPU_PREC_C64 ? sizeof(float2) : sizeof(double2));
+    const size_t smem = s.prec == SGPU_PREC_C64 ? UvwGeom<float>::smem : UvwGeom<double>::smem;
     if (smem > 48 * 1024) {  // set on every call: the attribute is per device
       e = s.prec == SGPU_PREC_C64
               ? cudaFuncSetAttribute(k_uvpsi_w<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
               : cudaFuncSetAttribute(k_uvpsi_w<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (e != cudaSuccess) return e;
     }
-    const dim3 gu(s.nitems, s.nkl);
+    const dim3 gu(s.nitems, s.nkl, (s.NBocc + 31) / 32);
     // the compact sphere values are current after every Taylor step: 4x fewer bytes than gathering from zu
     const bool fromS = s.S_valid && s.Sbuf;
     const int ld = fromS ? s.nsp : s.NL;
@@ -551,11 +574,11 @@ cudaError_t launch_current(System& s, double* jav_dev) {
     if (s.prec == SGPU_PREC_C64)
       k_uvpsi_w<float><<<gu, 256, smem, s.launch_stream()>>>(fromS ? (const float2*)s.Sbuf : (const float2*)s.zu, ld,
                                                               s.NBocc, s.zproj64, s.Nlma, s.Nps, idx, s.atom_off,
-                                                              s.rpos, s.items, s.lma_list, chunk, s.Uw);
+                                                              s.rpos, s.items, s.lma_list, s.Uw);
     else
       k_uvpsi_w<double><<<gu, 256, smem, s.launch_stream()>>>(fromS ? (const double2*)s.Sbuf : (const double2*)s.zu,
                                                                ld, s.NBocc, s.zproj64, s.Nlma, s.Nps, idx, s.atom_off,
-                                                               s.rpos, s.items, s.lma_list, chunk, s.Uw);
+                                                               s.rpos, s.items, s.lma_list, s.Uw);
   }
   k_current_comb<<<(s.norb + 127) / 128, 128, 0, s.launch_stream()>>>(part, nx, s.Uw, s.occ_o, s.kAc_d, s.iuV_d,
                                                                      s.norb, s.NBocc, s.Nlma, s.Hxyz, 1.0 / s.aLxyz,
