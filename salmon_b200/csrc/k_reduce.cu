@@ -533,6 +533,11 @@ static cudaError_t current_stencil(System& s, const Nab12& nab, const double* na
     nx = s.cur_fixed == 2 ? 2 : 4;
     return s.cur_fixed == 2 ? current_march_yh<R, 32, 32, 2>(s, nab, part) : current_march_yh<R, 32, 32, 4>(s, nab, part);
   }
+  // 48x48 planes (the 48^3 grid): six CTAs of 8 rows (384 threads) per orbital plane
+  if (s.cur_fixed && s.NLy == 48 && s.NLz == 48) {
+    nx = 6;
+    return current_march_yh<R, 48, 48, 6>(s, nab, part);
+  }
   if (NYZ <= 256) return current_march<R, 256, 1, 1>(s, nab, part);
   if (NYZ <= 512) return current_march<R, 512, 1, 1>(s, nab, part);
   if (NYZ <= 1024) return current_march<R, 1024, 1, 1>(s, nab, part);

@@ -26,6 +26,8 @@ CASES = {
     "microbench_16": lambda: S.microbench_system(16, nk_limit=1, Nb=32),
     # planes wider than one CTA (NLy*NLz/2 > 512): the pass splits them into y-blocks
     "wide_48": lambda: S.microbench_system(48, nk_limit=1, Nb=4),
+    # the compile-time 32x32 forms of the pass and of the current stencil
+    "microbench_32": lambda: S.microbench_system(32, nk_limit=1, Nb=4),
     "wide_ragged": lambda: S.small_system(6, 50, 22, nk=2, nb=3, a=(5.0, 12.0, 9.0), seed=23),
 }
 
