@@ -285,8 +285,9 @@ enum {
   SGPU_PARAM_PASS_FIXED = 6,  /* stencil pass, complex(4): 1 uses the compile-time plane shapes
                                  (16x16, 16x32, 20x20, 32x32 planes, 48x48 in three y-blocks: 9-plane
                                  ring, constant offsets) where they fit, 0 the generic kernel         */
-  SGPU_PARAM_CUR_FIXED = 7    /* current stencil: 1 splits each 32x32 plane over four CTAs (48x48:
-                                 six), 2 32x32 planes over two, 0 the generic kernels               */
+  SGPU_PARAM_CUR_FIXED = 7    /* current and energy stencils: 1 splits each 32x32 plane over four
+                                 CTAs (48x48: six), 2 32x32 planes of the current over two, 0 the
+                                 generic kernels                                                     */
 };
 
 /* CG preconditioners.  PLAIN is the reference's CG_ompk.  TPA multiplies the

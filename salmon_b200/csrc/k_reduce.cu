@@ -666,15 +666,86 @@ __global__ void __launch_bounds__(256, 2) k_ekin_plane(const C2<R>* __restrict__
   }
 }
 
+// The energy stencil as an x-march (GY x GZ planes split over NP CTAs of GY/NP
+// rows, one point per thread): psi at planes x-4..x+4 in a register queue
+// (FP64, converted once), plane x staged in FP64 in shared memory with four halo
+// rows on each side for the +-y neighbours.  The FD coefficients are kernel
+// parameters; k enters through nabt = k_d nab_d.  part[o][h][2].
+struct EkinCoef {
+  double lap0_2;     // -(lapx(0)+lapy(0)+lapz(0))/2
+  double lapt[12];   // lapx(1:4), lapy(1:4), lapz(1:4)
+  double nab[12];    // nabx(1:4), naby(1:4), nabz(1:4)
+};
+
+template <typename R, int GY, int GZ, int NP>
+__global__ void __launch_bounds__(GY / NP * GZ) k_ekin_march_yh(const C2<R>* __restrict__ zu, int NLx, int NBocc,
+                                                               const double* __restrict__ kAc, const EkinCoef c,
+                                                               double* __restrict__ out) {
+  constexpr int NYH = GY / NP, NT = NYH * GZ, NYZ = GY * GZ, RB = (NYH + 8) * GZ;
+  static_assert(NT % 32 == 0 && NT <= 1024 && 8 * GZ <= NT, "one point per thread, halos loaded by the first rows");
+  __shared__ double2 buf[2][RB];
+  __shared__ double sh[32 * 2];
+  const int o = blockIdx.x / NP, h = blockIdx.x - (blockIdx.x / NP) * NP, t = threadIdx.x;
+  const int kl = o / NBocc;
+  const C2<R>* E = zu + (size_t)o * NLx * NYZ;
+  double nabt[12];
+#pragma unroll
+  for (int n = 0; n < 12; ++n) nabt[n] = kAc[3 * kl + n / 4] * c.nab[n];
+  const int yl = t / GZ, z = t - (t / GZ) * GZ;
+  const int y0 = h * NYH;
+  const int own = (y0 + yl) * GZ + z;
+  // halo rows of threads t < 8 GZ: rows y0-4..y0-1 then y0+NYH..y0+NYH+3
+  const int hr = t / GZ;
+  const int hrow = hr < 4 ? (y0 - 4 + hr + GY) % GY : (y0 + NYH + hr - 4) % GY;
+  const int hdst = (hr < 4 ? hr : NYH + hr) * GZ + z;
+  const int hsrc = hrow * GZ + z;
+  double2 q[9];  // q[m]: plane x-4+m
+#pragma unroll
+  for (int m = 0; m < 9; ++m) q[m] = to_d2(__ldg(E + (size_t)((m - 4 + 4 * NLx) % NLx) * NYZ + own));
+  C2<R> nxt = __ldg(E + (size_t)(5 % NLx) * NYZ + own);
+  double v2[2] = {0, 0};
+  for (int x = 0; x < NLx; ++x) {
+    double2* pl = buf[x & 1];
+    pl[(4 + yl) * GZ + z] = q[4];
+    if (t < 8 * GZ) pl[hdst] = to_d2(__ldg(E + (size_t)x * NYZ + hsrc));
+    __syncthreads();
+    const double2 e = q[4];
+    double2 v = make_double2(0, 0), w = make_double2(0, 0);
+#pragma unroll
+    for (int n = 1; n <= 4; ++n) {
+      const double2 a1 = q[4 + n], a2 = q[4 - n];
+      const double2 b1 = pl[(4 + yl + n) * GZ + z], b2 = pl[(4 + yl - n) * GZ + z];
+      const double2 c1 = pl[(4 + yl) * GZ + (z + n) % GZ], c2 = pl[(4 + yl) * GZ + (z - n + GZ) % GZ];
+      v.x += c.lapt[n - 1] * (a1.x + a2.x) + c.lapt[3 + n] * (b1.x + b2.x) + c.lapt[7 + n] * (c1.x + c2.x);
+      v.y += c.lapt[n - 1] * (a1.y + a2.y) + c.lapt[3 + n] * (b1.y + b2.y) + c.lapt[7 + n] * (c1.y + c2.y);
+      w.x += nabt[n - 1] * (a1.x - a2.x) + nabt[3 + n] * (b1.x - b2.x) + nabt[7 + n] * (c1.x - c2.x);
+      w.y += nabt[n - 1] * (a1.y - a2.y) + nabt[3 + n] * (b1.y - b2.y) + nabt[7 + n] * (c1.y - c2.y);
+    }
+    // z = A e - 0.5 v - i w ;  F += conj(e) z
+    const double2 zz = make_double2(c.lap0_2 * e.x - 0.5 * v.x + w.y, c.lap0_2 * e.y - 0.5 * v.y - w.x);
+    v2[0] += e.x * zz.x + e.y * zz.y;
+    v2[1] += e.x * zz.y - e.y * zz.x;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) q[m] = q[m + 1];
+    q[8] = to_d2(nxt);
+    nxt = __ldg(E + (size_t)((x + 6) % NLx) * NYZ + own);
+  }
+  block_sum<2>(v2, sh);
+  if (t == 0) {
+    out[2 * (size_t)blockIdx.x] = v2[0];
+    out[2 * (size_t)blockIdx.x + 1] = v2[1];
+  }
+}
+
 // per orbital: occ Re(tpsum) Hxyz + occ |k|^2/2 and occ sum |U|^2 iuV
-__global__ void k_energy_comb(const double* __restrict__ part, int NLx, const double2* __restrict__ U,
+__global__ void k_energy_comb(const double* __restrict__ part, int nx, const double2* __restrict__ U,
                               const double* __restrict__ occ_o, const double* __restrict__ kAc,
                               const int* __restrict__ iuV, int norb, int NBocc, int Nlma, double Hxyz,
                               double* __restrict__ eo) {
   const int o = blockIdx.x * blockDim.x + threadIdx.x;
   if (o >= norb) return;
   double tr = 0;
-  for (int x = 0; x < NLx; ++x) tr += part[((size_t)o * NLx + x) * 2];
+  for (int x = 0; x < nx; ++x) tr += part[((size_t)o * nx + x) * 2];  // per-orbital rows, in order
   const int kl = o / NBocc;
   const double occ = occ_o[o];
   const double k2 = kAc[3 * kl] * kAc[3 * kl] + kAc[3 * kl + 1] * kAc[3 * kl + 1] + kAc[3 * kl + 2] * kAc[3 * kl + 2];
@@ -715,14 +786,40 @@ cudaError_t launch_energy(System& s, double* e_dev) {
     }
   cudaError_t err = cudaMemcpyAsync(coef, h, sizeof(h), cudaMemcpyHostToDevice, s.stream);
   if (err != cudaSuccess) return err;
-  const int gp = s.norb * s.NLx;
-  const int bt = s.NLy >= 8 ? 256 : 32 * s.NLy;
-  if (s.prec == SGPU_PREC_C64)
-    k_ekin_plane<float><<<gp, bt, 0, s.launch_stream()>>>((const float2*)s.zu, s.NLx, s.NLy, s.NLz, s.NBocc, s.kAc_d,
-                                                          coef, part);
-  else
-    k_ekin_plane<double><<<gp, bt, 0, s.launch_stream()>>>((const double2*)s.zu, s.NLx, s.NLy, s.NLz, s.NBocc, s.kAc_d,
-                                                           coef, part);
+  int nx = s.NLx;
+  EkinCoef ec;
+  ec.lap0_2 = h[0];
+  for (int k = 0; k < 12; ++k) {
+    ec.lapt[k] = h[1 + k];
+    ec.nab[k] = h[13 + k];
+  }
+  // 32x32 and 48x48 planes: the x-march over planes split in 8-row parts (SGPU_PARAM_CUR_FIXED)
+  if (s.cur_fixed && s.NLy == 32 && s.NLz == 32) {
+    nx = 4;
+    if (s.prec == SGPU_PREC_C64)
+      k_ekin_march_yh<float, 32, 32, 4><<<4 * s.norb, 256, 0, s.launch_stream()>>>((const float2*)s.zu, s.NLx, s.NBocc,
+                                                                                   s.kAc_d, ec, part);
+    else
+      k_ekin_march_yh<double, 32, 32, 4><<<4 * s.norb, 256, 0, s.launch_stream()>>>((const double2*)s.zu, s.NLx,
+                                                                                    s.NBocc, s.kAc_d, ec, part);
+  } else if (s.cur_fixed && s.NLy == 48 && s.NLz == 48) {
+    nx = 6;
+    if (s.prec == SGPU_PREC_C64)
+      k_ekin_march_yh<float, 48, 48, 6><<<6 * s.norb, 384, 0, s.launch_stream()>>>((const float2*)s.zu, s.NLx, s.NBocc,
+                                                                                   s.kAc_d, ec, part);
+    else
+      k_ekin_march_yh<double, 48, 48, 6><<<6 * s.norb, 384, 0, s.launch_stream()>>>((const double2*)s.zu, s.NLx,
+                                                                                    s.NBocc, s.kAc_d, ec, part);
+  } else {
+    const int gp = s.norb * s.NLx;
+    const int bt = s.NLy >= 8 ? 256 : 32 * s.NLy;
+    if (s.prec == SGPU_PREC_C64)
+      k_ekin_plane<float><<<gp, bt, 0, s.launch_stream()>>>((const float2*)s.zu, s.NLx, s.NLy, s.NLz, s.NBocc, s.kAc_d,
+                                                            coef, part);
+    else
+      k_ekin_plane<double><<<gp, bt, 0, s.launch_stream()>>>((const double2*)s.zu, s.NLx, s.NLy, s.NLz, s.NBocc,
+                                                             s.kAc_d, coef, part);
+  }
   err = cudaGetLastError();
   if (err != cudaSuccess) return err;
   // U = Hxyz * sum conj(zproj) psi = Hxyz * sum uV ekr psi  (total_energy.f90:191-197), FP64 projectors
@@ -730,7 +827,7 @@ cudaError_t launch_energy(System& s, double* e_dev) {
     err = launch_uvpsi(s, s.zu, 0, s.norb, s.NBocc, false);
     if (err != cudaSuccess) return err;
   }
-  k_energy_comb<<<(s.norb + 127) / 128, 128, 0, s.launch_stream()>>>(part, s.NLx, s.U, s.occ_o, s.kAc_d, s.iuV_d,
+  k_energy_comb<<<(s.norb + 127) / 128, 128, 0, s.launch_stream()>>>(part, nx, s.U, s.occ_o, s.kAc_d, s.iuV_d,
                                                                     s.norb, s.NBocc, s.Nlma, s.Hxyz, eo);
   k_energy_sum<<<1, 256, 0, s.launch_stream()>>>(eo, s.norb, e_dev);
   return cudaGetLastError();
