@@ -92,6 +92,133 @@ module salmon_gpu
       real(c_double), intent(in)  :: kac(*)
       real(c_double), intent(out) :: ekin, enl
     end function
+    ! ---- precision, device state, streams
+    integer(c_int) function sgpu_set_precision(h, precision) bind(C, name="sgpu_set_precision")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int), value :: precision
+    end function
+    integer(c_int) function sgpu_synchronize(h) bind(C, name="sgpu_synchronize")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+    type(c_ptr) function sgpu_stream(h) bind(C, name="sgpu_stream")
+      import :: c_ptr
+      type(c_ptr), value :: h
+    end function
+    type(c_ptr) function sgpu_state_ptr(h) bind(C, name="sgpu_state_ptr")
+      import :: c_ptr
+      type(c_ptr), value :: h
+    end function
+    integer(c_int) function sgpu_set_state_dev(h, zu_dev) bind(C, name="sgpu_set_state_dev")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h, zu_dev      ! device address (OpenACC host_data use_device)
+    end function
+    integer(c_int) function sgpu_hpsi_batch(h, ikb_s, ikb_e, tpsi, htpsi) bind(C, name="sgpu_hpsi_batch")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int), value :: ikb_s, ikb_e
+      type(c_ptr), value :: tpsi, htpsi    ! device addresses in the handle's precision
+    end function
+    ! ---- self-consistent local potential (RT/dt_evolve.f90:190-207)
+    integer(c_int) function sgpu_set_vpsl(h, vpsl) bind(C, name="sgpu_set_vpsl")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h
+      real(c_double), intent(in) :: vpsl(*)
+    end function
+    integer(c_int) function sgpu_update_vloc(h, rho, eh_exc) bind(C, name="sgpu_update_vloc")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+      type(c_ptr), value :: rho            ! c_loc(rho) after the allreduce, or c_null_ptr
+      type(c_ptr), value :: eh_exc         ! c_loc(e(2)) for (Eh, Exc), or c_null_ptr
+    end function
+    integer(c_int) function sgpu_get_vloc(h, vloc) bind(C, name="sgpu_get_vloc")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h
+      real(c_double), intent(out) :: vloc(*)
+    end function
+    ! ---- ground state (GS/*), FP64
+    integer(c_int) function sgpu_gs_set_state(h, zu_gs) bind(C, name="sgpu_gs_set_state")
+      import :: c_int, c_ptr, c_double_complex
+      type(c_ptr), value :: h
+      complex(c_double_complex), intent(in) :: zu_gs(*)
+    end function
+    integer(c_int) function sgpu_gs_get_state(h, zu_gs) bind(C, name="sgpu_gs_get_state")
+      import :: c_int, c_ptr, c_double_complex
+      type(c_ptr), value :: h
+      complex(c_double_complex), intent(out) :: zu_gs(*)
+    end function
+    integer(c_int) function sgpu_gram_schmidt(h) bind(C, name="sgpu_gram_schmidt")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+    integer(c_int) function sgpu_cg(h, ncg, esp_var, iters) bind(C, name="sgpu_cg")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int), value :: ncg
+      type(c_ptr), value :: esp_var, iters ! c_loc(esp_var(NB,NK_s:NK_e)) / c_loc(iters) or c_null_ptr
+    end function
+    integer(c_int) function sgpu_set_cg_delta(h, delta_cg) bind(C, name="sgpu_set_cg_delta")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h
+      real(c_double), value :: delta_cg
+    end function
+    integer(c_int) function sgpu_cg_residuals(h, res) bind(C, name="sgpu_cg_residuals")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h
+      real(c_double), intent(out) :: res(*)
+    end function
+    integer(c_int) function sgpu_subspace_diag(h, esp) bind(C, name="sgpu_subspace_diag")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h
+      real(c_double), intent(out) :: esp(*)
+    end function
+    integer(c_int) function sgpu_gs_to_rt(h) bind(C, name="sgpu_gs_to_rt")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+    ! ---- tuning and timing
+    integer(c_int) function sgpu_set_param(h, param, val) bind(C, name="sgpu_set_param")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int), value :: param, val
+    end function
+    integer(c_int) function sgpu_get_param(h, param, val) bind(C, name="sgpu_get_param")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int), value :: param
+      integer(c_int), intent(out) :: val
+    end function
+    integer(c_int) function sgpu_autotune(h, reps, nslab, split, ms_per_apply) bind(C, name="sgpu_autotune")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h
+      integer(c_int), value :: reps
+      integer(c_int), intent(out) :: nslab, split
+      real(c_double), intent(out) :: ms_per_apply
+    end function
+    integer(c_int) function sgpu_time_kernel(h, kernel, reps, ms) bind(C, name="sgpu_time_kernel")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h
+      integer(c_int), value :: kernel, reps
+      real(c_double), intent(out) :: ms
+    end function
+    ! ---- several systems in one CUDA-graph replay
+    integer(c_int) function sgpu_batch_create(handles, n, b) bind(C, name="sgpu_batch_create")
+      import :: c_int, c_ptr
+      type(c_ptr), intent(in) :: handles(*)
+      integer(c_int), value :: n
+      type(c_ptr), intent(out) :: b
+    end function
+    integer(c_int) function sgpu_batch_step(b, dt, nsteps) bind(C, name="sgpu_batch_step")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: b
+      real(c_double), intent(in) :: dt(*)
+      integer(c_int), value :: nsteps
+    end function
+    integer(c_int) function sgpu_batch_destroy(b) bind(C, name="sgpu_batch_destroy")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: b
+    end function
   end interface
 
 contains
@@ -131,6 +258,27 @@ contains
     d%uV = c_loc(uV); d%iuV = c_loc(iuV); d%a_tbl = c_loc(a_tbl); d%occ = c_loc(occ)
     call sgpu_check(sgpu_create(d, int(precision, c_int), sgpu_h), 'sgpu_create')
     call sgpu_check(sgpu_set_state(sgpu_h, zu_t), 'sgpu_set_state')   ! !$acc enter data copyin(zu_t)
+  end subroutine
+
+  ! The ground-state sequence of one SCF iteration (control/ground_state.f90:135-139) on the
+  ! device copy of zu_GS: Gram_Schmidt, diag_omp, Gram_Schmidt, CG_omp(Ncg), Gram_Schmidt.
+  ! Load zu_GS once with sgpu_gs_set_state; esp and esp_var come back FP64.
+  subroutine gpu_gs_iteration(ncg_in, esp_out, esp_var_out)
+    use global_variables, only: NB, NK_s, NK_e
+    integer, intent(in) :: ncg_in
+    real(8), intent(out), target :: esp_out(NB, NK_s:NK_e), esp_var_out(NB, NK_s:NK_e)
+    call sgpu_check(sgpu_gram_schmidt(sgpu_h), 'sgpu_gram_schmidt')
+    call sgpu_check(sgpu_subspace_diag(sgpu_h, esp_out), 'sgpu_subspace_diag')
+    call sgpu_check(sgpu_gram_schmidt(sgpu_h), 'sgpu_gram_schmidt')
+    call sgpu_check(sgpu_cg(sgpu_h, int(ncg_in, c_int), c_loc(esp_var_out), c_null_ptr), 'sgpu_cg')
+    call sgpu_check(sgpu_gram_schmidt(sgpu_h), 'sgpu_gram_schmidt')
+  end subroutine
+
+  ! Drop-in for psi_rho_RT + Hartree + Exc_Cor + Vloc = Vh + Vpsl + Vexc after the step
+  ! (RT/dt_evolve.f90:190-207), on the device; rho after comm_summation is passed in.
+  subroutine gpu_update_vloc(rho_in)
+    real(8), intent(in), target :: rho_in(:)
+    call sgpu_check(sgpu_update_vloc(sgpu_h, c_loc(rho_in), c_null_ptr), 'sgpu_update_vloc')
   end subroutine
 
   ! Drop-in for update_projector(kac) (common/projector.f90:29)
