@@ -58,3 +58,25 @@ def test_create_rejects_bad_descriptor():
     d = sysm.desc()
     rc = _lib.lib().sgpu_create(C.byref(d), 7, C.byref(h))
     assert rc == -1
+
+
+def test_fortran_binding_names_exist():
+    """Every bind(C, name="...") of fortran/salmon_gpu_iface.f90 (the module a
+    SALMON maintainer adds; not compiled here) names an entry point the header
+    declares and the library exports, and the descriptor type lists the fields
+    of sgpu_desc in the header's order."""
+    from salmon_b200 import build
+    text = open(os.path.join(ROOT, "fortran", "salmon_gpu_iface.f90")).read()
+    bound = sorted(set(re.findall(r'bind\(C,\s*name="(sgpu_\w+)"\)', text)))
+    assert len(bound) >= 30
+    declared = set(declared_symbols())
+    lib = C.CDLL(build.build())
+    assert [n for n in bound if n not in declared or not hasattr(lib, n)] == []
+    ftype = re.search(r"type, bind\(C\) :: sgpu_desc(.*?)end type", text, re.S).group(1)
+    fnames = [n.strip().split("(")[0].lower() for line in ftype.splitlines() if "::" in line
+              for n in line.split("::")[1].split(",") if n.strip()]
+    htext = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "salmon_gpu.h")).read(), flags=re.S)
+    hdesc = re.search(r"typedef struct sgpu_desc\s*\{(.*?)\}\s*sgpu_desc;", htext, re.S).group(1)
+    hnames = [n.strip().split("[")[0].lower() for decl in hdesc.split(";") if decl.strip()
+              for n in re.sub(r"\b(const|int32_t|double|int)\b|\*", " ", decl).split(",") if n.strip()]
+    assert fnames == hnames, (fnames, hnames)
