@@ -59,6 +59,8 @@ def parse():
     p.add_argument("--batched-steps", type=int, default=1000)
     p.add_argument("--no-large", action="store_true", help="skip the Si216 48^3 run")
     p.add_argument("--precond", action="store_true", help="also run the Si64 CG preconditioner comparison (minutes)")
+    p.add_argument("--pass-fixed", type=int, default=1, choices=[0, 1],
+                   help="stencil pass of the main leg: 1 compile-time plane shapes where they apply, 0 the generic kernel")
     p.add_argument("--profile-current", action="store_true",
                    help="profiling: one complex(4) Taylor step of the workload, then two sgpu_current calls, and exit")
     p.add_argument("--kb-kernel", type=int, default=0, choices=[0, 1, 2],
@@ -452,6 +454,7 @@ def main():
         g.set_vloc(vloc)
         g.update_projector(kAc)
         g.set_param("kb_kernel", args.kb_kernel)
+        g.set_param("pass_fixed", args.pass_fixed)
         stream = torch.cuda.ExternalStream(g.stream)
         for _ in range(args.warmup):
             g.hamiltonian(DT)
