@@ -181,3 +181,32 @@ def test_gs_wfn_files_round_trip_and_layout(tmp_path):
     (tmp_path / "gs_wfn_k" / "wfn_gs_k0000003.wfn").write_bytes(raw[:-2])
     with pytest.raises(ValueError):
         wfn_io.read_gs_wfn_k(str(tmp_path), NK, NB, NL)
+
+
+def test_d_projectors_with_s_local():
+    """With the s channel local (lloc = 0) the p and d channels carry projectors:
+    3 + 5 per atom.  The atoms sit on grid points of the 8^3 grid, so each sphere
+    is cubic-symmetric and projectors of different (l, m) are orthogonal on it; the
+    d functions follow the Ylm table (e.g. r^2 Y_20 ~ (3z^2 - r^2)/2)."""
+    t = P.prepare(P.from_npz(os.path.join(GOLDEN, "si_rps_ky.npz"), lloc=0))
+    assert list(t.inorm[1:] != 0) == [True, True] and t.inorm[0] == 0
+    sysm, kAc0, vpsl, zu = S.si_pp_system(t, with_orbitals=False)
+    assert sysm.Nlma == 8 * 8 and list(sysm.a_tbl[:9]) == [1] * 8 + [2]
+    m = int(sysm.Mps[0])
+    u = sysm.uV[:8, :m]
+    gram = u @ u.T
+    assert np.abs(gram - np.diag(np.diag(gram))).max() < 1e-12 * np.abs(gram).max()
+    # r^2 Y_20 ~ (3z^2 - r^2)/2 times a radial factor: zero where 3z^2 = r^2, and the
+    # ratio to (3z^2 - r^2) depends on r only
+    _, _, _, _, _, dist = S.calc_jxyz(8, 8, 8, sysm.aL, sysm.Rion, t.pp.rps)
+    x, y, z = dist[0, :m, 0], dist[0, :m, 1], dist[0, :m, 2]
+    d0 = u[3 + 2]                                            # l = 2, m = 0 (after the three p)
+    ang = 3 * z * z - (x * x + y * y + z * z)
+    scale = np.abs(d0).max()
+    zero = np.abs(ang) < 1e-9
+    assert zero.any() and np.abs(d0[zero]).max() < 1e-12 * scale
+    r = np.round(np.sqrt(x * x + y * y + z * z), 9)
+    for rr in np.unique(r[~zero]):
+        sel = (~zero) & (r == rr)
+        ratio = d0[sel] / ang[sel]
+        assert np.abs(ratio - ratio[0]).max() <= 1e-12 * np.abs(ratio).max()
