@@ -203,6 +203,14 @@ module salmon_gpu
       real(c_double), intent(out) :: ms
     end function
     ! ---- several systems in one CUDA-graph replay
+    ! occ: pass occ(1,NK_s) with ld_occ = NB; zu, occ and rho are device
+    ! addresses (inside !$acc host_data use_device(zu_t, occ, rho))
+    integer(c_int) function sgpu_psi_rho_static(precision, NL, nb, nk, zu, occ, ld_occ, rho, stream) &
+        bind(C, name="sgpu_psi_rho_static")
+      import :: c_int, c_ptr
+      integer(c_int), value :: precision, NL, nb, nk, ld_occ
+      type(c_ptr), value    :: zu, occ, rho, stream
+    end function
     integer(c_int) function sgpu_batch_create(handles, n, b) bind(C, name="sgpu_batch_create")
       import :: c_int, c_ptr
       type(c_ptr), intent(in) :: handles(*)

@@ -201,13 +201,19 @@ int sgpu_psi_rho(sgpu_handle h, double* rho_l);
  * orbitals the CALLER keeps on the device: zu(NL,nb,nk) complex(8)
  * (precision SGPU_PREC_C128) or complex(4) (SGPU_PREC_C64), occ and rho
  * device arrays; enqueued on `stream` (a cudaStream_t, NULL = the legacy
- * default stream) and not waited for.  Needs no handle and allocates no
+ * default stream) and not waited for.  occ is indexed from the caller's first
+ * local k-point: a rank holding k-points NK_s..NK_e of the reference's
+ * occ(NB,NK) passes the device address of occ(1,NK_s) with ld_occ = NB (in
+ * OpenACC Fortran: `!$acc host_data use_device(zu_t, occ, rho)` around the
+ * call, with occ(1,NK_s) as the argument).  Needs no handle and allocates no
  * device memory: its scratch is a static device array of
  * SGPU_PSI_RHO_STATIC_SCRATCH_DOUBLES doubles, and larger problems are
  * rejected with SGPU_ERR_ARG.  It is meant for hosts that own the orbitals
  * through their own device runtime and cannot allocate at that point.
- * The first call on each device looks up the scratch address
- * (cudaGetSymbolAddress), so make it before capturing any stream.  All calls
+ * The scratch address is looked up once per CUDA context
+ * (cudaGetSymbolAddress, keyed on the context's ID, so a device reset or a
+ * host-created context gets a fresh lookup); the first call in a context may
+ * load the library's device code, so make it before capturing any stream.  All calls
  * on one device share the scratch: calls whose executions overlap race, so
  * order them (one stream, or events).
  * No counterpart in the reference; the computation is psi_rho_impl with

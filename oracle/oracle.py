@@ -25,14 +25,29 @@ _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
 
 
+# Where the SALMON source tree is read from: the REF_ROOT environment variable,
+# else this recipe's one default location (the same default as oracle/Makefile).
+# Only the recipes (this build, the Makefile, tests/golden/*.py) read the tree;
+# machines without it use the prebuilt _ref library and the committed fixtures.
+_REF_ROOT_DEFAULT = "/root/reference"
+
+
+def ref_root():
+    """The SALMON source tree, or None when it is not present on this machine."""
+    root = os.environ.get("REF_ROOT") or _REF_ROOT_DEFAULT
+    return root if os.path.isdir(os.path.join(root, "src", "ARTED")) else None
+
+
 def build(quiet=True):
     """Builds liboracle.so, and _ref/libsalmon_ref.so when the reference tree
     is present (oracle/Makefile)."""
     targets = ["liboracle.so"]
-    ref_root = os.environ.get("REF_ROOT", "/root/reference")
-    if os.path.isdir(os.path.join(ref_root, "src", "ARTED", "stencil", "C", "AVX")):
+    env = dict(os.environ)
+    root = ref_root()
+    if root and os.path.isdir(os.path.join(root, "src", "ARTED", "stencil", "C", "AVX")):
         targets.append("ref")
-    out = subprocess.run(["make", "-C", HERE] + targets, capture_output=True, text=True)
+        env["REF_ROOT"] = root
+    out = subprocess.run(["make", "-C", HERE] + targets, capture_output=True, text=True, env=env)
     if out.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
     if not quiet:

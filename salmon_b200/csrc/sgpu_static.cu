@@ -23,19 +23,17 @@
 #include <cstdint>
 #include <mutex>
 #include <string>
+#include <utility>
+#include <vector>
 
 #include "sgpu_internal.cuh"
 
 namespace {
 
-constexpr int kChunk = 64;       // orbitals per partial density (the handle path uses the same split)
-constexpr int kMaxDevices = 64;  // device ordinals the set-up table covers
+constexpr int kChunk = 64;  // orbitals per partial density (the handle path uses the same split)
 
 // The scratch: ceil(norb / kChunk) partial densities of NL values each.
 static __device__ __align__(256) double g_rho_scratch[SGPU_PSI_RHO_STATIC_SCRATCH_DOUBLES];
-
-std::mutex g_setup_mu;
-double* g_scratch_of_device[kMaxDevices] = {};
 
 // Partial density of orbitals [o0, o0 + kChunk) at grid point i, accumulated
 // in FP64 in orbital order; orbital o = ib + nb * ik has weight occ[ib + ld_occ * ik].
@@ -65,25 +63,56 @@ __global__ void k_rho_sum_static(const double* __restrict__ part, int nchunk, in
 
 int reject(int code, std::string msg);
 
-// Device address of the scratch on the current device, looked up once per
-// device (cudaGetSymbolAddress may load the library's device code, which is
-// why the first call on a device should not be made inside stream capture).
-int scratch_for_current_device(double** out) {
-  int dev = -1;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return reject(SGPU_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-  if (dev < 0 || dev >= kMaxDevices)
-    return reject(SGPU_ERR_UNSUPPORTED, "device ordinal " + std::to_string(dev) + " is beyond the set-up table (" +
-                                            std::to_string(kMaxDevices) + " devices)");
+// Set-up: the device address of the scratch, looked up with
+// cudaGetSymbolAddress once per context and kept in a small table.  In host code
+// the name g_rho_scratch is only a host-side stand-in, never a device address.
+// The table is keyed on the unique ID of the CURRENT CUDA context, not on the
+// device ordinal: an address belongs to the context it was taken in, so after a
+// device reset, or when a host runtime makes its own non-primary context
+// current, the first call in that context looks the address up again instead of
+// reusing a stale one.  The context ID comes from the driver's cuCtxGetCurrent
+// and cuCtxGetId (IDs are never reused within a process), reached through
+// cudaGetDriverEntryPoint so that the library does not link libcuda; where that
+// fails the address is looked up on every call.  A lookup allocates nothing, but
+// the first one in a context may load the library's device code into it, which
+// is why the first call in a context must not be made inside stream capture.
+using CtxGetCurrentFn = int (*)(void**);
+using CtxGetIdFn = int (*)(void*, unsigned long long*);
+std::mutex g_setup_mu;
+std::vector<std::pair<unsigned long long, double*>> g_scratch_of_context;
+
+template <typename F>
+F driver_fn(const char* name) {
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint(name, &fn, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess)
+    return nullptr;
+  return reinterpret_cast<F>(fn);
+}
+
+int scratch_for_current_context(double** out) {
+  static const CtxGetCurrentFn ctx_get_current = driver_fn<CtxGetCurrentFn>("cuCtxGetCurrent");
+  static const CtxGetIdFn ctx_get_id = driver_fn<CtxGetIdFn>("cuCtxGetId");
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  const bool keyed = ctx_get_current && ctx_get_id && ctx_get_current(&ctx) == 0 && ctx != nullptr &&
+                     ctx_get_id(ctx, &id) == 0;
   std::lock_guard<std::mutex> lock(g_setup_mu);
-  if (!g_scratch_of_device[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_rho_scratch);
-    if (e != cudaSuccess || !p)
-      return reject(SGPU_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
-    g_scratch_of_device[dev] = static_cast<double*>(p);
+  if (keyed)
+    for (const auto& e : g_scratch_of_context)
+      if (e.first == id) {
+        *out = e.second;
+        return 0;
+      }
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_rho_scratch);
+  if (e != cudaSuccess || !p)
+    return reject(SGPU_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+  *out = static_cast<double*>(p);
+  if (keyed) {
+    if (g_scratch_of_context.size() >= 256) g_scratch_of_context.clear();  // bounded; entries are only a cache
+    g_scratch_of_context.emplace_back(id, *out);
   }
-  *out = g_scratch_of_device[dev];
   return 0;
 }
 
@@ -114,7 +143,7 @@ extern "C" int sgpu_psi_rho_static(int precision, int NL, int nb, int nk, const 
                                     std::to_string(kChunk) + ") x NL); the static maximum is " +
                                     std::to_string((long long)SGPU_PSI_RHO_STATIC_SCRATCH_DOUBLES));
   double* part = nullptr;
-  if (int rc = scratch_for_current_device(&part)) return rc;
+  if (int rc = scratch_for_current_context(&part)) return rc;
   // Nothing in the scratch has to start at zero: every partial density row
   // that k_rho_sum_static reads is written in full by k_rho_partial_static
   // earlier on the same stream, so no clearing pass is needed.

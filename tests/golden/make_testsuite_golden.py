@@ -80,7 +80,9 @@ def parse_rps(path):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REF_ROOT")
+    if not ref:
+        sys.exit("usage: make_testsuite_golden.py <SALMON source tree>  (or set REF_ROOT)")
     ts = os.path.join(ref, "testsuites")
     d = parse_rps(os.path.join(ts, "pseudo", "Si_rps.dat"))
     np.savez_compressed(os.path.join(HERE, "si_rps_ky.npz"), **d)

@@ -14,7 +14,6 @@ import pytest
 from _helpers import GOLDEN
 from salmon_b200 import broyden, drive, pseudo as P, system as S
 
-REF_RPS = "/root/reference/testsuites/pseudo/Si_rps.dat"
 
 
 def _si():
@@ -27,9 +26,11 @@ def _suite():
 
 
 def test_fixture_matches_reader():
-    if not os.path.exists(REF_RPS):
-        pytest.skip("reference tree not present")
-    a = P.read_ps_ky(REF_RPS, lloc=2)
+    from oracle import oracle as O
+    root = O.ref_root()
+    if root is None:
+        pytest.skip("reference tree not present (set REF_ROOT)")
+    a = P.read_ps_ky(os.path.join(root, "testsuites", "pseudo", "Si_rps.dat"), lloc=2)
     b = _si()
     assert a.mr == b.mr and a.zps == b.zps == 4 and a.mlps == b.mlps == 2
     assert np.array_equal(a.vpp, b.vpp) and np.array_equal(a.upp, b.upp) and np.array_equal(a.rrc, b.rrc)
