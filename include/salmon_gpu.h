@@ -372,7 +372,7 @@ int sgpu_batch_destroy(sgpu_batch_handle b);
 /* Kernels that sgpu_time_kernel can time. */
 enum {
   SGPU_KERNEL_STENCIL_PASS = 0, /* one H application of every resident orbital (zu -> workspace)     */
-  SGPU_KERNEL_TAYLOR_LAST = 1,  /* the fused last Taylor pass (H application + update), on workspace */
+  SGPU_KERNEL_TAYLOR_LAST = 1,  /* one Taylor stage (H application + update psi + c H psi), on workspace */
   SGPU_KERNEL_UVPSI = 2,        /* the Kleinman-Bylander projections of every resident orbital       */
   SGPU_KERNEL_PSI_RHO = 3,      /* the density reduction                                             */
   SGPU_KERNEL_KB_FIELD = 4,     /* the Kleinman-Bylander term at the sphere points from the projections */

@@ -25,17 +25,15 @@
 #include <type_traits>
 
 #include "sgpu_internal.cuh"
+#include "stencil_ops.cuh"
 
 namespace sgpu {
 
 template <typename R>
 struct PassArgs {
   const C2<R>* in;       // [nb][NL]
-  C2<R>* out;            // [nb][NL]   (modes 0,1)
+  C2<R>* out;            // [nb][NL]
   C2<R>* tt;             // [nb][NL]   (mode 1)
-  const C2<R>* t1;       // [nb][NL]   (mode 2)
-  const C2<R>* t2;
-  C2<R>* zu;             // [nb][NL]   (mode 2, read and written)
   const R* vloc;
   const double* kAc;     // [nkl][3]
   int o_beg, NBocc;
@@ -57,102 +55,8 @@ struct PassArgs {
   const C2<R>* W;        // [nb][nsp] KB term at the sphere points (null: none)
   C2<R>* S;              // [nb][nsp] export of the output (null: none)
   int nsp, maxpts;
-  C2<R> zf[4];
+  C2<R> zf;              // mode 2: the Taylor stage coefficient c
 };
-
-// ------------------------------------------------------------- helpers ---
-// asynchronous copy of N complex elements (8- or 16-byte aligned runs)
-template <typename R, int N>
-__device__ __forceinline__ void cp_run(C2<R>* dst, const C2<R>* src) {
-  constexpr int BYTES = N * (int)sizeof(C2<R>);
-  if constexpr (BYTES == 8) {
-    cp_async8(dst, src);
-  } else {
-#pragma unroll
-    for (int k = 0; k < BYTES / 16; ++k)
-      cp_async16(reinterpret_cast<char*>(dst) + 16 * k, reinterpret_cast<const char*>(src) + 16 * k);
-  }
-}
-
-template <typename R, int RZ>
-__device__ __forceinline__ void ld_run(C2<R> (&d)[RZ], const C2<R>* p) {
-  if constexpr (RZ == 2 && std::is_same<R, float>::value) {
-    const float4 t = __ldg(reinterpret_cast<const float4*>(p));
-    d[0] = make_float2(t.x, t.y);
-    d[1] = make_float2(t.z, t.w);
-  } else {
-#pragma unroll
-    for (int r = 0; r < RZ; ++r) d[r] = __ldg(p + r);
-  }
-}
-template <typename R, int RZ>
-__device__ __forceinline__ void ld_run_rw(C2<R> (&d)[RZ], const C2<R>* p) {
-  if constexpr (RZ == 2 && std::is_same<R, float>::value) {
-    const float4 t = *reinterpret_cast<const float4*>(p);
-    d[0] = make_float2(t.x, t.y);
-    d[1] = make_float2(t.z, t.w);
-  } else {
-#pragma unroll
-    for (int r = 0; r < RZ; ++r) d[r] = p[r];
-  }
-}
-template <typename R, int RZ>
-__device__ __forceinline__ void st_run(C2<R>* p, const C2<R> (&d)[RZ]) {
-  if constexpr (RZ == 2 && std::is_same<R, float>::value) {
-    *reinterpret_cast<float4*>(p) = make_float4(d[0].x, d[0].y, d[1].x, d[1].y);
-  } else {
-#pragma unroll
-    for (int r = 0; r < RZ; ++r) p[r] = d[r];
-  }
-}
-template <typename R, int RZ>
-__device__ __forceinline__ void lds_run(C2<R> (&d)[RZ], const C2<R>* p) {
-  if constexpr (RZ == 2 && std::is_same<R, float>::value) {
-    const float4 t = *reinterpret_cast<const float4*>(p);
-    d[0] = make_float2(t.x, t.y);
-    d[1] = make_float2(t.z, t.w);
-  } else {
-#pragma unroll
-    for (int r = 0; r < RZ; ++r) d[r] = p[r];
-  }
-}
-// the RZ local sphere indices of this thread's points (-1: not a sphere point)
-template <int RZ>
-__device__ __forceinline__ void ld_lq(int (&d)[RZ], const short* p) {
-  if constexpr (RZ == 2) {
-    const int v = __ldg(reinterpret_cast<const int*>(p));
-    d[0] = (int)(short)(v & 0xffff);
-    d[1] = v >> 16;
-  } else {
-    d[0] = __ldg(p);
-  }
-}
-
-__device__ __forceinline__ int wrapi(int a, int n) { a %= n; return a < 0 ? a + n : a; }
-
-// v += cl (p + m), wa += cn (p - m).  Complex(4) runs on packed FP32 pairs
-// (sm_100 f32x2 add/fma: one instruction updates both parts of a complex
-// value; cl, cn are broadcast pairs); complex(8) on scalar FP64.
-__device__ __forceinline__ void stencil_pair(float2& v, float2& wa, float2 p, float2 m, float2 cl, float2 cn) {
-  const float2 sum = __fadd2_rn(p, m);
-  const float2 dif = __ffma2_rn(m, make_float2(-1.f, -1.f), p);  // p - m (exact negation)
-  v = __ffma2_rn(cl, sum, v);
-  wa = __ffma2_rn(cn, dif, wa);
-}
-__device__ __forceinline__ void stencil_pair(double2& v, double2& wa, double2 p, double2 m, double cl, double cn) {
-  v.x = fma(cl, p.x + m.x, v.x);
-  v.y = fma(cl, p.y + m.y, v.y);
-  wa.x = fma(cn, p.x - m.x, wa.x);
-  wa.y = fma(cn, p.y - m.y, wa.y);
-}
-template <typename R> __device__ __forceinline__ auto kpair(double k) {
-  if constexpr (std::is_same<R, float>::value) return make_float2((float)k, (float)k); else return k;
-}
-// w = k wa (first axis) or w += k wa
-__device__ __forceinline__ float2 kscale(float2 k, float2 wa, float2 w) { return __ffma2_rn(k, wa, w); }
-__device__ __forceinline__ double2 kscale(double k, double2 wa, double2 w) {
-  return make_double2(fma(k, wa.x, w.x), fma(k, wa.y, w.y));
-}
 
 template <typename R> struct PassGeom {
   static constexpr int NR = std::is_same<R, float>::value ? 8 : 6;  // ring planes
@@ -170,7 +74,9 @@ size_t pass_smem_bytes(int prec, int NLy, int NLz, int maxpts, bool with_w, int 
 }
 
 // MODE 0: out = H in.   MODE 1: also tt = H in - V in before the nonlocal term.
-// MODE 2: zu = zu + zf0 t1 + zf1 t2 + zf2 in + zf3 H in   (RT/hamiltonian.f90:99-122).
+// MODE 2: out = in + c H in, one linear factor of the Taylor polynomial
+// (RT/hamiltonian.f90:46-49, :99-122 evaluated as the product of its four
+// linear factors; see enqueue_taylor_step).
 //
 // YB (planes of more than 512 threads' points): the plane is split over nyblk
 // CTAs of NYB rows; each CTA's ring holds its rows and 4 halo rows on each side.
@@ -409,10 +315,9 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
       }
 #pragma unroll
       for (int r = 0; r < RZ; ++r) { w[r] = kscale(kz, wa[r], mk<R>(0, 0)); wa[r] = mk<R>(0, 0); }
-      // the y terms go to a second accumulator (fixed shapes, H application): two
-      // shorter FMA chains (0.469 -> 0.438 ms at 32^3; the last Taylor pass, at 128
-      // registers, is 2% slower with it and keeps one accumulator)
-      constexpr bool SPLITV = FIXED && MODE != 2;
+      // the y terms go to a second accumulator (fixed shapes): two shorter FMA
+      // chains (0.469 -> 0.438 ms at 32^3)
+      constexpr bool SPLITV = FIXED;
       T vy[RZ];
 #pragma unroll
       for (int r = 0; r < RZ; ++r) vy[r] = mk<R>(0, 0);
@@ -455,24 +360,11 @@ __global__ void __launch_bounds__(512) k_hpsi_pass(const PassArgs<R> a) {
         if (with_w && lq[r] >= 0) f = cadd(f, wpl[lq[r]]);  // + pseudo_pt scatter (hpsi.f90:203-206)
         res[r] = f;
       }
-      if constexpr (MODE == 2) {  // update (RT/hamiltonian.f90:114-117)
-        T ps[RZ], p1[RZ], p2[RZ];
-        ld_run_rw<R, RZ>(ps, a.zu + (size_t)b * a.NL + pbase);
-        ld_run<R, RZ>(p1, a.t1 + (size_t)b * a.NL + pbase);
-        ld_run<R, RZ>(p2, a.t2 + (size_t)b * a.NL + pbase);
+      if constexpr (MODE == 2) {  // one Taylor stage: out = in + c H in
 #pragma unroll
-        for (int r = 0; r < RZ; ++r) {
-          T u = ps[r];
-          u = cfma(a.zf[0], p1[r], u);
-          u = cfma(a.zf[1], p2[r], u);
-          u = cfma(a.zf[2], q[(P + 4) % 9][r], u);
-          u = cfma(a.zf[3], res[r], u);
-          res[r] = u;
-        }
-        st_run<R, RZ>(a.zu + (size_t)b * a.NL + pbase, res);
-      } else {
-        st_run<R, RZ>(a.out + (size_t)b * a.NL + pbase, res);
+        for (int r = 0; r < RZ; ++r) res[r] = cfma(a.zf, res[r], q[(P + 4) % 9][r]);
       }
+      st_run<R, RZ>(a.out + (size_t)b * a.NL + pbase, res);
       if (do_export) {  // the output at the sphere points, for the next projections
         const int q0 = YB ? spo[x * (nyblk + 1)] : spo[x];
 #pragma unroll
@@ -562,9 +454,6 @@ static cudaError_t launch_pass_t(const System& s, const PassIO& io, int o_beg, i
   a.in = (const C2<R>*)io.in;
   a.out = (C2<R>*)io.out;
   a.tt = (C2<R>*)io.tt;
-  a.t1 = (const C2<R>*)io.t1;
-  a.t2 = (const C2<R>*)io.t2;
-  a.zu = (C2<R>*)io.zu;
   a.vloc = std::is_same<R, float>::value ? (const R*)s.vloc32 : (const R*)s.vloc64;
   a.kAc = s.kAc_d;
   a.o_beg = o_beg;
@@ -589,7 +478,7 @@ static cudaError_t launch_pass_t(const System& s, const PassIO& io, int o_beg, i
   a.S = (C2<R>*)io.S;
   a.nsp = s.nsp;
   a.maxpts = s.maxpts;
-  for (int n = 0; n < 4; ++n) a.zf[n] = mk<R>((R)io.zfac[n][0], (R)io.zfac[n][1]);
+  a.zf = mk<R>((R)io.zc[0], (R)io.zc[1]);
   const int nthr = a.NYB * (s.NLz / RZ);
   const int block = ((nthr + 31) / 32) * 32;
   const bool tb = pass_tables(s, RZ);

@@ -230,20 +230,20 @@ cudaError_t launch_kb_term(const System& s, const void* in, bool from_S, int o_b
 size_t pass_smem_bytes(int prec, int NLy, int NLz, int maxpts, bool with_w, int NLx, int nyblk = 1, int NYB = 0,
                        bool tables = false, int nr = 0);
 
-// One H application: out = H in  (mode 0), with ttpsi (mode 1), or the last
-// Taylor pass (mode 2): zu = zu + z1 t1 + z2 t2 + z3 in + z4 H in.  U must hold
-// the projections of `in` (launch_uvpsi with scale_iuv=true).
+// One H application: out = H in  (mode 0), with ttpsi (mode 1), or one stage
+// of the Taylor step (mode 2): out = in + c H in.  W must hold the KB term of
+// `in` (launch_kb_term).
 struct PassIO {
   const void* in = nullptr;
   void* out = nullptr;
   void* tt = nullptr;
-  const void* t1 = nullptr;
-  const void* t2 = nullptr;
-  void* zu = nullptr;
   const void* W = nullptr;         // KB term at the sphere points ([nb][nsp]) or null (no projectors)
   void* S = nullptr;               // export of the output at the sphere points ([nb][nsp]) or null
-  double zfac[4][2] = {};
+  double zc[2] = {0.0, 0.0};       // mode 2: the stage coefficient c (re, im)
 };
+// The four stage coefficients of a 4th-order Taylor step of length dt:
+// 1 + sum_{n=1..4} (-i dt H)^n / n! = prod_{s=0..3} (1 + c_s H).
+void taylor_stage_coefs(double dt, double c[4][2]);
 // prec = -1 uses the handle's precision; SGPU_PREC_C128 forces FP64 (ground state).
 cudaError_t launch_hpsi_pass(const System& s, int mode, const PassIO& io, int o_beg, int nb, int nbk, int prec = -1);
 // threads per CTA of the pass kernel for an NLy x NLz plane
