@@ -63,6 +63,9 @@ def parse():
                    help="stencil pass of the main leg: 1 compile-time plane shapes where they apply, 0 the generic kernel")
     p.add_argument("--profile-current", action="store_true",
                    help="profiling: one complex(4) Taylor step of the workload, then two sgpu_current calls, and exit")
+    p.add_argument("--taylor-kernel", type=int, default=0, choices=[0, 1, 2],
+                   help="Taylor step of the main leg: 0 by grid, 1 stencil passes, 2 shared-memory resident")
+    p.add_argument("--no-si8", action="store_true", help="skip the Si8 16^3 resident-vs-passes leg")
     p.add_argument("--kb-kernel", type=int, default=0, choices=[0, 1, 2],
                    help="KB term kernel of the main leg: 0 by grid size, 1 band-group tile, 2 band-quad (profiling)")
     return p.parse_args()
@@ -455,6 +458,7 @@ def main():
         g.update_projector(kAc)
         g.set_param("kb_kernel", args.kb_kernel)
         g.set_param("pass_fixed", args.pass_fixed)
+        g.set_param("taylor_kernel", args.taylor_kernel)
         stream = torch.cuda.ExternalStream(g.stream)
         for _ in range(args.warmup):
             g.hamiltonian(DT)

@@ -168,8 +168,12 @@ int sgpu_update_projector(sgpu_handle h, const double* kAc);
 /* One 4th-order Taylor step of every resident orbital:
  *   zu <- zu + sum_{n=1..4} ((-i dt)^n / n!) H^n zu,
  * with H built from the last sgpu_update_projector / sgpu_set_vloc.
- * flag_current is accepted for argument compatibility and ignored (the
- * reference ignores it unless built with ARTED_CURRENT_PREPROCESSING).
+ * flag_current non-zero also computes the stencil part of the current of the
+ * new orbitals (sum |psi|^2 and the current_stencil sums, which do not depend
+ * on k+A), as the reference does under ARTED_CURRENT_PREPROCESSING
+ * (current_omp_KB_ST after the update, RT/hamiltonian.f90:68-70); a following
+ * sgpu_current on the unchanged orbitals uses them instead of re-reading the
+ * orbitals (current.f90:154-156, :213-224).
  * Replaces hamiltonian(zu,flag_current) (RT/hamiltonian.f90:27-123). */
 int sgpu_hamiltonian(sgpu_handle h, double dt, int flag_current);
 
@@ -291,9 +295,14 @@ enum {
   SGPU_PARAM_PASS_FIXED = 6,  /* stencil pass, complex(4): 1 uses the compile-time plane shapes
                                  (16x16, 16x32, 20x20, 32x32 planes, 48x48 in three y-blocks: 9-plane
                                  ring, constant offsets) where they fit, 0 the generic kernel         */
-  SGPU_PARAM_CUR_FIXED = 7    /* current and energy stencils: 1 splits each 32x32 plane over four
+  SGPU_PARAM_CUR_FIXED = 7,   /* current and energy stencils: 1 splits each 32x32 plane over four
                                  CTAs (48x48: six), 2 32x32 planes of the current over two, 0 the
                                  generic kernels                                                     */
+  SGPU_PARAM_TAYLOR_KERNEL = 8 /* Taylor step: 1 four stencil passes over all orbitals (any grid), 2
+                                 the orbitals of a band group resident in one CTA's shared memory for
+                                 the whole step (16x16, 16x32 and 20x20 planes where they fit), 0 the
+                                 resident form where it is the faster one (complex(4), 16x16 planes),
+                                 else the passes                                                     */
 };
 
 /* CG preconditioners.  PLAIN is the reference's CG_ompk.  TPA multiplies the

@@ -547,22 +547,37 @@ static cudaError_t current_stencil(System& s, const Nab12& nab, const double* na
   return cudaGetLastError();
 }
 
-cudaError_t launch_current(System& s, double* jav_dev) {
-  double* part = s.red;                              // [norb][nx][4]
-  double* jo = part + (size_t)s.norb * s.NLx * 4;    // [norb][3]
-  double* nab12 = jo + 3 * (size_t)s.norb;           // [12]
+// The stencil sums {jt, F, G, H} of the resident orbitals into part[o][nx][4].
+// The 12 nab coefficients of the plane form live at the end of the handle's
+// reduction scratch.
+cudaError_t launch_current_stencil(System& s, double* part, int& nx) {
+  double* nab12 = s.red + (size_t)s.norb * s.NLx * 4 + 3 * (size_t)s.norb;  // [12]
   if ((size_t)s.norb * s.NLx * 4 + 3 * (size_t)s.norb + 12 > s.red_elems) return cudaErrorInvalidValue;
   double h[12];
   for (int n = 0; n < 4; ++n)
     for (int d = 0; d < 3; ++d) h[4 * d + n] = s.nab[d][n + 1];
-  cudaError_t e = cudaMemcpyAsync(nab12, h, sizeof(h), cudaMemcpyHostToDevice, s.stream);
-  if (e != cudaSuccess) return e;
   Nab12 nab;
   for (int k = 0; k < 12; ++k) nab.v[k] = h[k];
-  int nx = 1;
-  e = s.prec == SGPU_PREC_C64 ? current_stencil<float>(s, nab, nab12, part, nx)
-                              : current_stencil<double>(s, nab, nab12, part, nx);
+  nx = 1;
+  const cudaError_t e = cudaMemcpyAsync(nab12, h, sizeof(h), cudaMemcpyHostToDevice, s.stream);
   if (e != cudaSuccess) return e;
+  return s.prec == SGPU_PREC_C64 ? current_stencil<float>(s, nab, nab12, part, nx)
+                                 : current_stencil<double>(s, nab, nab12, part, nx);
+}
+
+cudaError_t launch_current(System& s, double* jav_dev) {
+  double* part = s.red;                              // [norb][nx][4]
+  double* jo = part + (size_t)s.norb * s.NLx * 4;    // [norb][3]
+  if ((size_t)s.norb * s.NLx * 4 + 3 * (size_t)s.norb + 12 > s.red_elems) return cudaErrorInvalidValue;
+  int nx = 1;
+  cudaError_t e;
+  if (s.cur_valid) {  // computed by the Taylor step that produced these orbitals (flag_current)
+    part = s.cur_part;
+    nx = s.cur_nx;
+  } else {
+    e = launch_current_stencil(s, part, nx);
+    if (e != cudaSuccess) return e;
+  }
   if (s.Nlma && s.nitems) {
     const size_t smem = s.prec == SGPU_PREC_C64 ? UvwGeom<float>::smem : UvwGeom<double>::smem;
     if (smem > 48 * 1024) {  // set on every call: the attribute is per device

@@ -139,8 +139,20 @@ void sgpu::taylor_stage_coefs(double dt, double c[4][2]) {
 // One Taylor step of every resident orbital, enqueued on the handle's stream
 // (kernel launches only, so it can be captured into a CUDA graph): four stages
 // zu -> tw0 -> tw1 -> tw0 -> zu.
-cudaError_t sgpu::enqueue_taylor_step(System& sys, double dt, bool gather_first) {
+cudaError_t sgpu::enqueue_taylor_step(System& sys, double dt, bool gather_first, bool with_current) {
   System* s = &sys;
+  s->cur_valid = false;
+  const bool resident = s->taylor_kernel == 2 || (s->taylor_kernel == 0 && sgpu::resident_step_default(*s));
+  if (resident) {
+    // the whole step on chip, a band group per CTA (it gathers its own projections)
+    cudaError_t e = sgpu::launch_taylor_resident(*s, s->zu, dt, with_current ? s->cur_part : nullptr,
+                                                 s->nsp > 0 ? s->Sbuf : nullptr);
+    if (e != cudaSuccess) return e;
+    s->S_valid = s->nsp > 0;
+    s->cur_nx = 1;
+    s->cur_valid = with_current;
+    return cudaSuccess;
+  }
   double c[4][2];
   taylor_stage_coefs(dt, c);
   // Each stage exports its output at the sphere points (S); the next stage's
@@ -160,6 +172,12 @@ cudaError_t sgpu::enqueue_taylor_step(System& sys, double dt, bool gather_first)
     if (e != cudaSuccess) return e;
   }
   s->S_valid = s->nsp > 0;
+  if (with_current) {  // the stencil sums of the new orbitals, right after the update
+    int nx = 1;
+    if ((e = sgpu::launch_current_stencil(*s, s->cur_part, nx)) != cudaSuccess) return e;
+    s->cur_nx = nx;
+    s->cur_valid = true;
+  }
   return cudaSuccess;
 }
 
@@ -402,6 +420,8 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
   s->red_elems = std::max<size_t>({nchunk * s->NL, 4 * (size_t)s->norb + 64, (size_t)s->NL + 64,
                                    sgpu::current_red_elems(s->norb, s->NLx)});
   if ((e = dalloc(&s->red, s->red_elems)) != cudaSuccess) return bail(cuda_fail(e, "alloc red"));
+  if ((e = dalloc(&s->cur_part, (size_t)s->norb * s->NLx * 4)) != cudaSuccess)
+    return bail(cuda_fail(e, "alloc cur_part"));
   s->red_h_elems = (size_t)s->NL + 64;
   if ((e = cudaMallocHost((void**)&s->red_h, s->red_h_elems * sizeof(double))) != cudaSuccess)
     return bail(cuda_fail(e, "alloc pinned"));
@@ -425,7 +445,7 @@ int sgpu_destroy(sgpu_handle h) {
   free_state_buffers(s);
   void* bufs[] = {s->vloc64, s->vloc32, s->occ_o, s->kAc_d, s->idx_proj, s->atom_off, s->rpos, s->items,
                   s->lma_list, s->iuV_d, s->lma_atom, s->uV_d, s->zproj64, s->zproj32, s->sp_off, s->rec, s->cont, s->qmap, s->kbq, s->kb_multi, s->lqi, s->Sbuf, s->Wbuf,
-                  s->U, s->Uw, s->red, s->stage};
+                  s->U, s->Uw, s->red, s->stage, s->cur_part};
   for (void* p : bufs) cudaFree(p);
   void* gbufs[] = {s->gs_zu, s->gs_aux, s->gs_W, s->gs_st, s->gs_part, s->gs_A, s->gs_V, s->gs_w, s->gs_sweeps,
                    s->occ_gs, s->gs_out, s->gs_res, s->gs_tb, s->vpsl, s->rho_d, s->exc_d, s->sp_blk};
@@ -463,6 +483,7 @@ int sgpu_set_state(sgpu_handle h, const double* zu) {
   CK(cudaStreamSynchronize(s->stream));
   s->have_state = true;
   s->S_valid = false;
+  s->cur_valid = false;
   return 0;
 }
 
@@ -477,6 +498,7 @@ int sgpu_set_state_dev(sgpu_handle h, const void* zu_dev) {
   CK(cudaStreamSynchronize(s->stream));
   s->have_state = true;
   s->S_valid = false;
+  s->cur_valid = false;
   return 0;
 }
 
@@ -510,6 +532,7 @@ int sgpu_set_precision(sgpu_handle h, int precision) {
   s->zu = nullptr;
   s->prec = precision;
   s->S_valid = false;
+  s->cur_valid = false;
   s->elem = precision == SGPU_PREC_C64 ? sizeof(float2) : sizeof(double2);
   CK(cudaMalloc(&s->zu, n * s->elem));
   if (s->have_state) {
@@ -547,12 +570,11 @@ int sgpu_update_projector(sgpu_handle h, const double* kAc) {
 }
 
 int sgpu_hamiltonian(sgpu_handle h, double dt, int flag_current) {
-  (void)flag_current;
   if (!valid(h)) return fail(SGPU_ERR_ARG, "null handle");
   System* s = h;
   if (!s->have_state || !s->have_vloc || !s->have_proj)
     return fail(SGPU_ERR_STATE, "sgpu_hamiltonian: state, Vloc and projectors must be set first");
-  CK(sgpu::enqueue_taylor_step(*s, dt, !s->S_valid));
+  CK(sgpu::enqueue_taylor_step(*s, dt, !s->S_valid, flag_current != 0));
   return 0;
 }
 
@@ -925,6 +947,7 @@ int sgpu_gs_to_rt(sgpu_handle h) {
   CK(cudaStreamSynchronize(s->stream));
   s->have_state = true;
   s->S_valid = false;
+  s->cur_valid = false;
   return 0;
 }
 
@@ -968,6 +991,13 @@ extern "C" int sgpu_set_param(sgpu_handle h, int param, int value) {
       s->pass_fixed = value;
       if (sgpu::prepare_pass(*s) != cudaSuccess) return fail(SGPU_ERR_CUDA, "sgpu_set_param: pass setup failed");
       return 0;
+    case SGPU_PARAM_TAYLOR_KERNEL:
+      if (value < 0 || value > 2) return fail(SGPU_ERR_ARG, "sgpu_set_param: Taylor kernel must be 0, 1 or 2");
+      if (value == 2 && !sgpu::resident_step_fits(*s))
+        return fail(SGPU_ERR_UNSUPPORTED, "sgpu_set_param: no shared-memory resident Taylor step for this grid");
+      s->taylor_kernel = value;
+      if (sgpu::prepare_resident(*s) != cudaSuccess) return fail(SGPU_ERR_CUDA, "sgpu_set_param: resident setup failed");
+      return 0;
     case SGPU_PARAM_LAUNCHES:
       if (value != 0) return fail(SGPU_ERR_ARG, "sgpu_set_param: the launch counter can only be reset to 0");
       s->launches = 0;
@@ -988,6 +1018,7 @@ extern "C" int sgpu_get_param(sgpu_handle h, int param, int* value) {
     case SGPU_PARAM_KB_KERNEL: *value = h->kb_kernel; return 0;
     case SGPU_PARAM_PASS_FIXED: *value = h->pass_fixed; return 0;
     case SGPU_PARAM_CUR_FIXED: *value = h->cur_fixed; return 0;
+    case SGPU_PARAM_TAYLOR_KERNEL: *value = h->taylor_kernel; return 0;
     default: return fail(SGPU_ERR_ARG, "sgpu_get_param: unknown parameter");
   }
 }

@@ -54,6 +54,7 @@ int capture(sgpu_batch* b, const double* dt, int nsteps) {
   for (System* s : b->sys) {
     if ((e = sgpu::prepare_pass(*s)) != cudaSuccess) return bcuda(e, "sgpu_batch_step: prepare");
     if ((e = sgpu::prepare_kb(*s)) != cudaSuccess) return bcuda(e, "sgpu_batch_step: prepare");
+    if ((e = sgpu::prepare_resident(*s)) != cudaSuccess) return bcuda(e, "sgpu_batch_step: prepare");
   }
   std::vector<unsigned long long> before(b->sys.size());
   for (size_t i = 0; i < b->sys.size(); ++i) before[i] = b->sys[i]->launches;
@@ -154,6 +155,7 @@ int sgpu_batch_step(sgpu_batch_handle b, const double* dt, int nsteps) {
   for (size_t i = 0; i < b->sys.size(); ++i) {
     b->sys[i]->launches += b->launches_per_replay[i];
     b->sys[i]->S_valid = b->sys[i]->nsp > 0;
+    b->sys[i]->cur_valid = false;
   }
   return 0;
 }

@@ -193,6 +193,13 @@ struct System {
   int pass_tab = 1;                // stencil pass: Vloc/sphere-index tables through the ring (two-point form)
   int pass_fixed = 1;              // stencil pass: compile-time plane shapes with a 9-plane ring (complex(4))
   int cur_fixed = 1;               // current stencil, 32x32 planes: 1 four CTAs per plane, 2 two, 0 one
+  int taylor_kernel = 0;           // Taylor step: 0 auto, 1 stencil passes, 2 the shared-memory resident kernel
+  // The current's stencil sums {jt, F, G, H} of the resident orbitals, computed by a
+  // Taylor step called with flag_current (RT/hamiltonian.f90:68-70): rows
+  // cur_part[o][cur_nx][4], valid while cur_valid (the orbitals are unchanged since).
+  double* cur_part = nullptr;      // [norb][NLx][4]
+  int cur_nx = 0;
+  bool cur_valid = false;
   int nsm = 148;                   // SMs of the device
   mutable bool kb_smem_ok = false;  // the KB tile kernels' shared-memory limits are raised for this handle
   int um_split = 4;                // band-quad KB kernel: warps splitting the points of one tile (1, 2, 4, 8)
@@ -317,7 +324,22 @@ void set_last_error(const std::string& msg);
 // One Taylor step of every resident orbital on the handle's stream (kernel
 // launches only).  gather_first: the first projections gather from the
 // orbitals instead of reading the sphere values S of the previous step.
-cudaError_t enqueue_taylor_step(System& s, double dt, bool gather_first);
+// with_current: also compute the current's stencil sums of the new orbitals
+// into cur_part (flag_current of RT/hamiltonian.f90:27).
+cudaError_t enqueue_taylor_step(System& s, double dt, bool gather_first, bool with_current = false);
+
+// The Taylor step with each orbital resident in one CTA's shared memory
+// (k_resident.cu): whether the handle's grid and precision have that form, the
+// launch (cur: [norb][4] stencil sums or null; S: sphere-value export or null),
+// and the shared-memory attribute (before a graph capture).
+// resident_step_default: the form the auto setting picks (where it measured faster).
+bool resident_step_fits(const System& s);
+bool resident_step_default(const System& s);
+cudaError_t launch_taylor_resident(const System& s, void* zu, double dt, double* cur, void* S);
+cudaError_t prepare_resident(const System& s);
+// The current's stencil sums of the resident orbitals into part[o][nx][4]
+// (k_reduce.cu; nx returned).
+cudaError_t launch_current_stencil(System& s, double* part, int& nx);
 
 }  // namespace sgpu
 
