@@ -4,7 +4,7 @@
 Workload: the hpsi/Taylor operator microbench (cubic Si-like cell a=10.26 bohr,
 grid 32^3 by default, 4x4x4 = 64 k-points, 32 bands, 8 atoms x {s,p} Gaussian
 Kleinman-Bylander projectors, seeded synthetic orbitals and V_loc).  A step is
-one Taylor step of every orbital (4 H applications + the update).  Both orbital
+one Taylor step of every orbital (4 H applications, each with its stage update).  Both orbital
 precisions run: complex(8) (FP64) and complex(4) orbitals with FP64
 reductions.  The headline `value` is the complex(4) path; the FP64 path is
 reported beside it.
@@ -35,10 +35,10 @@ sys.path.insert(0, ROOT)
 
 METRIC = "RT orbital-updates/s: FP32+FP64-reduce vs FP64 GPU at ΔJ<1e-5; hpsi %HBM peak"
 DT = 0.08
-# ncu dram__bytes_read.sum + dram__bytes_write.sum of one stencil-pass launch, per
-# orbital, from the capture in profiles/k_hpsi_pass_fixed32_c64_32cubed_864orb.md
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of one Taylor-stage launch, per
+# orbital, from the capture in profiles/k_hpsi_pass_stage_c64_32cubed_864orb.md
 # (864 orbitals; traffic grows with the orbital count).
-NCU_TRAFFIC_BYTES_PER_ORBITAL = {("stencil_pass", "c64", 32): 534.936064e6 / 864}
+NCU_TRAFFIC_BYTES_PER_ORBITAL = {("taylor_stage", "c64", 32): 534.936064e6 / 864}
 
 
 def parse():
@@ -371,6 +371,43 @@ def precond_bench(max_outer=60):
                         f"{max_outer} outer iterations)"}
 
 
+def si8_bench(nsteps=50):
+    """The Si8 RT shape of the plain FP64 run (16^3 grid, 4x4x4 k, 16 bands, 1024
+    orbitals; synthetic Gaussian projectors and V_loc): Taylor-step time of the
+    shared-memory resident form (the whole step in one kernel) against the four
+    stencil passes, in both orbital precisions."""
+    import torch
+    from salmon_b200 import system as S
+    from salmon_b200.rt import GpuSystem
+    sysm, kAc, vloc, zu = S.si_supercell_system((1, 1, 1), (16, 16, 16), (4, 4, 4), 16, A=(1e-2, 0.0, 0.0))
+    norb = sysm.nk_local * sysm.NBoccmax
+    out = {"workload": "Si8 16^3, 64 k x 16 bands (1024 orbitals), synthetic Gaussian projectors / V_loc"}
+    for prec in ("c64", "c128"):
+        r = {}
+        for name, tk in (("passes", 1), ("resident", 2)):
+            with GpuSystem(sysm, prec) as g:
+                g.set_state(zu)
+                g.set_vloc(vloc)
+                g.update_projector(kAc)
+                g.set_param("taylor_kernel", tk)
+                st = torch.cuda.ExternalStream(g.stream)
+                for _ in range(5):
+                    g.hamiltonian(DT)
+                g.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                for _ in range(nsteps):
+                    g.hamiltonian(DT)
+                e1.record(st)
+                e1.synchronize()
+                ms = e0.elapsed_time(e1) / nsteps
+                r[name] = {"ms_per_step": ms, "orbital_updates_per_s": norb / (ms * 1e-3)}
+        r["resident_speedup"] = r["passes"]["ms_per_step"] / r["resident"]["ms_per_step"]
+        out[prec] = r
+    return out
+
+
 def bench_config(args, sysm, norb, world):
     """The `config` of both arms' JSON lines (the same workload description)."""
     return {"workload": f"hpsi/Taylor microbench {args.grid}^3, {sysm.NK} k x {sysm.NBoccmax} bands per GPU",
@@ -491,7 +528,8 @@ def main():
         t_kb = g.time_kernel("kb_field", reps=10)
         t_kbt = g.time_kernel("kb_term", reps=10)
         alg = 2.0 * S_bytes * NL * norb  # algorithmic bytes of one H application over all orbitals
-        r.update(t_pass_ms=t_pass, t_last_ms=t_last, t_uvpsi_ms=t_uv, t_kb_ms=t_kb, t_kbterm_ms=t_kbt, achieved_gbs=alg / (t_pass * 1e-3) / 1e9,
+        r.update(t_pass_ms=t_pass, t_last_ms=t_last, t_uvpsi_ms=t_uv, t_kb_ms=t_kb, t_kbterm_ms=t_kbt,
+                 achieved_gbs=alg / (t_last * 1e-3) / 1e9, pass_gbs=alg / (t_pass * 1e-3) / 1e9,
                  step_gbs=10.0 * S_bytes * NL * norb / (r["ms_per_step"] * 1e-3) / 1e9)
         if args.no_e2e:
             res[prec] = r
@@ -504,7 +542,7 @@ def main():
             kt = kA + np.array([0.0, 0.0, 1e-4 * it])[:, None]
             g.update_projector(kt)
             g.set_vloc(vloc)
-            g.hamiltonian(DT)
+            g.hamiltonian(DT, flag_current=True)  # the current's stencil sums with the step
             rho = g.psi_rho_RT()
             jav = g.current_RT(kt)
             if world > 1:  # comm_summation of rho and J (psi_rho.f90:88, current.f90:286) over NCCL
@@ -529,6 +567,9 @@ def main():
     large = None
     if rank == 0 and not (args.only or args.no_e2e or args.no_large):
         large = large_bench()
+    si8 = None
+    if rank == 0 and not (args.only or args.no_e2e or args.no_si8):
+        si8 = si8_bench()
     pc = precond_bench() if (rank == 0 and args.precond) else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -540,7 +581,7 @@ def main():
         print(json.dumps({p: {k: v for k, v in r.items() if k != "e2e"} for p, r in res.items()}))
     elif rank == 0:
         h = res["c64"]
-        tpo = NCU_TRAFFIC_BYTES_PER_ORBITAL.get(("stencil_pass", "c64", args.grid))
+        tpo = NCU_TRAFFIC_BYTES_PER_ORBITAL.get(("taylor_stage", "c64", args.grid))
         traffic = tpo * norb if tpo else None
         out = {
             "metric": METRIC, "value": h["value"], "unit": "orbital-updates/s", "n_gpus": world, "steps": args.steps,
@@ -548,16 +589,16 @@ def main():
             "vs_baseline": None, "dtype": "c64 orbitals (FP32 stencil), FP64 reductions", "data": "synthetic",
             "config": bench_config(args, sysm, norb, world),
             "fp64_path": {"value": res["c128"]["value"], "ms_per_step": res["c128"]["ms_per_step"],
-                          "e2e": res["c128"]["e2e"], "stencil_pass_ms": res["c128"]["t_pass_ms"],
-                          "stencil_pass_gbs": res["c128"]["achieved_gbs"]},
+                          "e2e": res["c128"]["e2e"], "taylor_stage_ms": res["c128"]["t_last_ms"],
+                          "taylor_stage_gbs": res["c128"]["achieved_gbs"]},
             "fp32_over_fp64": h["value"] / res["c128"]["value"],
-            "kernels_ms": {p: {"stencil_pass": res[p]["t_pass_ms"], "taylor_last": res[p]["t_last_ms"],
+            "kernels_ms": {p: {"stencil_pass (H only)": res[p]["t_pass_ms"], "taylor_stage": res[p]["t_last_ms"],
                                "kb_term (in the step)": res[p]["t_kbterm_ms"], "uvpsi alone": res[p]["t_uvpsi_ms"],
                                "kb_field alone": res[p]["t_kb_ms"]} for p in res},
             "step_gbs_algorithmic": {p: res[p]["step_gbs"] for p in res},
             "roofline": {"bound": "hbm", "achieved": h["achieved_gbs"], "peak": hbm_peak, "unit": "GB/s",
                          "frac": h["achieved_gbs"] / hbm_peak, "traffic": traffic,
-                         "kernel": "k_hpsi_pass<float,2,0> (one H application, all orbitals)",
+                         "kernel": "k_hpsi_pass<float,2,2> (one Taylor stage psi + c H psi, all orbitals)",
                          "peak_kind": peak_kind},
             "cpu_baseline": cpu,
             "e2e": h["e2e"],
@@ -565,6 +606,7 @@ def main():
             "precision": prec_check,
             "batched": batched,
             "large": large,
+            "si8_resident_vs_passes": si8,
             "precond": pc,
             "clocks": clocks,
         }
