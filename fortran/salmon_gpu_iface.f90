@@ -211,6 +211,14 @@ module salmon_gpu
       integer(c_int), value :: precision, NL, nb, nk, ld_occ
       type(c_ptr), value    :: zu, occ, rho, stream
     end function
+    integer(c_int) function sgpu_vloc_history_reset(h) bind(C, name="sgpu_vloc_history_reset")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+    integer(c_int) function sgpu_vloc_extrapolate(h) bind(C, name="sgpu_vloc_extrapolate")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
     integer(c_int) function sgpu_batch_create(handles, n, b) bind(C, name="sgpu_batch_create")
       import :: c_int, c_ptr
       type(c_ptr), intent(in) :: handles(*)

@@ -158,6 +158,20 @@ int sgpu_update_vloc(sgpu_handle h, const double* rho, double* eh_exc);
 /* device -> HOST Vloc(NL) (FP64). */
 int sgpu_get_vloc(sgpu_handle h, double* vloc);
 
+/* The enforced-time-reversal-symmetry (etrs) propagator's potential history on
+ * the device.  sgpu_vloc_history_reset sets Vloc_old(:,1) = Vloc_old(:,2) =
+ * Vloc at the start of a real-time run (control/control_sc.f90:82).
+ * sgpu_vloc_extrapolate, between the two half steps of dt_evolve_etrs_omp_KB,
+ * replaces Vloc by 3 Vloc - 3 Vloc_old(:,1) + Vloc_old(:,2) and shifts the
+ * history (Vloc_old(:,2) = Vloc_old(:,1), Vloc_old(:,1) = the previous Vloc)
+ * (RT/dt_evolve.f90:248-252).  A step of the etrs propagator is then
+ *   sgpu_update_projector(kAc(t)); sgpu_hamiltonian(dt/2, 0);
+ *   sgpu_vloc_extrapolate; sgpu_update_projector(kAc(t+dt));
+ *   sgpu_hamiltonian(dt/2, 1); sgpu_update_vloc(NULL)
+ * (RT/dt_evolve.f90:218-348 for the LDA functionals). */
+int sgpu_vloc_history_reset(sgpu_handle h);
+int sgpu_vloc_extrapolate(sgpu_handle h);
+
 /* ---- hot path ------------------------------------------------------------ */
 
 /* Sets k+A(t) for the following hpsi/hamiltonian calls and rebuilds the

@@ -58,6 +58,8 @@ ABI = {
     "sgpu_net_grad": (C.c_int, [_vp, _vp, _vp, _ip, _vp, _dp]),
     "sgpu_net_train_step": (C.c_int, [_vp, _vp, _vp, _ip, C.c_float, _dp]),
     "sgpu_autotune": (C.c_int, [_vp, _ip, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]),
+    "sgpu_vloc_history_reset": (C.c_int, [_vp]),
+    "sgpu_vloc_extrapolate": (C.c_int, [_vp]),
     "sgpu_batch_create": (C.c_int, [C.POINTER(C.c_void_p), _ip, C.POINTER(C.c_void_p)]),
     "sgpu_batch_step": (C.c_int, [_vp, _vp, _ip]),
     "sgpu_batch_stream": (C.c_void_p, [_vp]),

@@ -103,4 +103,32 @@ cudaError_t launch_update_vloc(const System& s, const double* rho_dev, double* e
   return cudaGetLastError();
 }
 
+// The etrs potential history (RT/dt_evolve.f90:248-252, control/control_sc.f90:82):
+// reset: hist1 = hist2 = Vloc;
+// extrapolate: Vnew = 3 Vloc - 3 hist1 + hist2, hist2 = hist1, hist1 = Vloc, Vloc = Vnew
+// (in FP64, with the FP32 copy of Vloc refreshed).
+__global__ void k_vloc_history(double* __restrict__ v64, float* __restrict__ v32, double* __restrict__ h1,
+                               double* __restrict__ h2, int NL, int extrapolate) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < NL; i += gridDim.x * blockDim.x) {
+    const double v = v64[i];
+    if (extrapolate) {
+      const double vn = 3.0 * v - 3.0 * h1[i] + h2[i];
+      h2[i] = h1[i];
+      h1[i] = v;
+      v64[i] = vn;
+      v32[i] = (float)vn;
+    } else {
+      h1[i] = v;
+      h2[i] = v;
+    }
+  }
+}
+
+cudaError_t launch_vloc_history(const System& s, bool extrapolate) {
+  if (!s.vloc_hist) return cudaErrorInvalidValue;
+  k_vloc_history<<<(s.NL + 255) / 256, 256, 0, s.launch_stream()>>>(s.vloc64, s.vloc32, s.vloc_hist,
+                                                                     s.vloc_hist + s.NL, s.NL, extrapolate ? 1 : 0);
+  return cudaGetLastError();
+}
+
 }  // namespace sgpu

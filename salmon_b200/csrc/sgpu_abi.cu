@@ -448,7 +448,8 @@ int sgpu_destroy(sgpu_handle h) {
                   s->U, s->Uw, s->red, s->stage, s->cur_part};
   for (void* p : bufs) cudaFree(p);
   void* gbufs[] = {s->gs_zu, s->gs_aux, s->gs_W, s->gs_st, s->gs_part, s->gs_A, s->gs_V, s->gs_w, s->gs_sweeps,
-                   s->occ_gs, s->gs_out, s->gs_res, s->gs_tb, s->vpsl, s->rho_d, s->exc_d, s->sp_blk};
+                   s->occ_gs, s->gs_out, s->gs_res, s->gs_tb, s->vpsl, s->rho_d, s->exc_d, s->sp_blk,
+                   s->vloc_hist};
   for (void* p : gbufs) cudaFree(p);
   if (s->gs_h) cudaFreeHost(s->gs_h);
   if (s->red_h) cudaFreeHost(s->red_h);
@@ -894,6 +895,23 @@ int sgpu_update_vloc(sgpu_handle h, const double* rho, double* eh_exc) {
   if (eh_exc) CK(cudaMemcpyAsync(eh_exc, s->exc_d, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   s->have_vloc = true;
+  return 0;
+}
+
+int sgpu_vloc_history_reset(sgpu_handle h) {
+  if (!valid(h)) return fail(SGPU_ERR_ARG, "null handle");
+  System* s = h;
+  if (!s->have_vloc) return fail(SGPU_ERR_STATE, "sgpu_vloc_history_reset: no Vloc set");
+  if (!s->vloc_hist) CK(cudaMalloc(&s->vloc_hist, 2 * (size_t)s->NL * sizeof(double)));
+  CK(sgpu::launch_vloc_history(*s, false));
+  return 0;
+}
+
+int sgpu_vloc_extrapolate(sgpu_handle h) {
+  if (!valid(h)) return fail(SGPU_ERR_ARG, "null handle");
+  System* s = h;
+  if (!s->vloc_hist) return fail(SGPU_ERR_STATE, "sgpu_vloc_extrapolate: call sgpu_vloc_history_reset first");
+  CK(sgpu::launch_vloc_history(*s, true));
   return 0;
 }
 

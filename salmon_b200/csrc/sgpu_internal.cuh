@@ -213,6 +213,7 @@ struct System {
   double* rho_d = nullptr;         // [NL] density used by the last potential update
   double* exc_d = nullptr;         // [2] Hartree and exchange-correlation energies
   double* gs_res = nullptr;        // [nkl][NB] residual norms of the last sgpu_cg
+  double* vloc_hist = nullptr;     // [2][NL] the etrs potential history Vloc_old(:,1:2) (allocated on first use)
 };
 
 // ------------------------------------------------------------ kernel API --
@@ -308,6 +309,9 @@ cudaError_t launch_precond_net(const System& s, double2* data, int nvec);
 // (Eh, Exc).  Grid sizes 2^a 3^b <= 96.
 cudaError_t launch_update_vloc(const System& s, const double* rho_dev, double* energies_dev);
 void net_free(System& s);
+// The etrs potential history: reset (both entries = Vloc) or extrapolate
+// (Vloc <- 3 Vloc - 3 hist1 + hist2, history shifted) on the device.
+cudaError_t launch_vloc_history(const System& s, bool extrapolate);
 cudaError_t launch_fft3d(const System& s, double2* data, int nvec, int sign, bool normalise);
 cudaError_t launch_tpa(const System& s, double2* data, int nvec, const double* tband_dev, int vecs_per_k,
                        const int* kidx_dev = nullptr);

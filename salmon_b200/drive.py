@@ -10,7 +10,9 @@ the device, sgpu_update_vloc):
   rt_propagate     control/control_sc.f90:150-230 with dt_evolve_omp_KB
                    'middlepoint' (RT/dt_evolve.f90:45-49, 176-207): k+A at the
                    midpoint for the Taylor step, then rho -> Vh + Vexc -> Vloc
-                   (scf=True), k+A(t+dt) for the current
+                   (scf=True), k+A(t+dt) for the current; or 'etrs'
+                   (dt_evolve_etrs_omp_KB, RT/dt_evolve.f90:218-348): two half steps
+                   around the extrapolated potential
   ground_state_scf the ground-state loop with the density mixed linearly between
                    iterations
   gs_scf           the reference's SCF loop: Broyden mixing (common/broyden.f90) and
@@ -150,19 +152,29 @@ def total_energy(g, sysm, kAc, vpsl, eion: float = 0.0):
 
 
 def rt_propagate(g, sysm, kAc0, vloc, Ac, dt: float, Nt: int, energy_every: int = 0, scf: bool = False,
-                 eion: float = 0.0):
-    """Nt middle-point Taylor steps of the resident orbitals; returns
+                 eion: float = 0.0, propagator: str = "middlepoint"):
+    """Nt Taylor-propagator steps of the resident orbitals; returns
     (javt (Nt+1,3) with javt[0] the current before the first step,
      energies {step: energy} every `energy_every` steps).
     scf=False: vloc is the fixed local potential (energies: band energy).
     scf=True: vloc is Vpsl; Vloc = Vh + Vpsl + Vexc is rebuilt from the density
-    after every step on the device (energies: total_energy)."""
+    after every step on the device (energies: total_energy).
+    propagator (dt_evolve_KB, RT/dt_evolve.f90:28-63):
+      'middlepoint'  one Taylor step of dt at k + (A(t) + A(t+dt))/2
+                     (dt_evolve_omp_KB, :104-207);
+      'etrs'         a half step dt/2 at k + A(t), the potential extrapolated to
+                     t + dt from its history (3 V - 3 V1 + V2), a half step dt/2 at
+                     k + A(t+dt) (dt_evolve_etrs_omp_KB, :218-348; LDA functionals)."""
+    if propagator not in ("middlepoint", "etrs"):
+        raise ValueError(f"invalid propagator {propagator!r}")
     kAc0 = np.ascontiguousarray(kAc0, dtype=np.float64)
     if scf:
         g.set_vpsl(vloc)
         g.update_vloc()
     else:
         g.set_vloc(vloc)
+    if propagator == "etrs":
+        g.vloc_history_reset()   # Vloc_old(:,1) = Vloc_old(:,2) = Vloc (control_sc.f90:82)
     energy = (lambda k: total_energy(g, sysm, k, vloc, eion)) if scf else (lambda k: band_energy(g, sysm, k, vloc))
     javt = np.zeros((Nt + 1, 3))
     javt[0] = g.current_RT(kAc0 + Ac[1][:, None])
@@ -170,9 +182,16 @@ def rt_propagate(g, sysm, kAc0, vloc, Ac, dt: float, Nt: int, energy_every: int 
     if energy_every:
         energies[0] = energy(kAc0 + Ac[1][:, None])
     for it in range(Nt):
-        kmid = kAc0 + 0.5 * (Ac[it + 1] + Ac[it + 2])[:, None]   # kAc0 + (Ac(it)+Ac(it+1))/2
-        g.update_projector(kmid)
-        g.hamiltonian(dt)
+        if propagator == "middlepoint":
+            kmid = kAc0 + 0.5 * (Ac[it + 1] + Ac[it + 2])[:, None]   # kAc0 + (Ac(it)+Ac(it+1))/2
+            g.update_projector(kmid)
+            g.hamiltonian(dt, flag_current=True)
+        else:
+            g.update_projector(kAc0 + Ac[it + 1][:, None])            # kAc = kAc0 + Ac_tot(iter)
+            g.hamiltonian(0.5 * dt)
+            g.vloc_extrapolate()                                      # dt_evolve.f90:248-252
+            g.update_projector(kAc0 + Ac[it + 2][:, None])            # kAc = kAc_new
+            g.hamiltonian(0.5 * dt, flag_current=True)
         if scf:
             g.update_vloc()       # psi_rho_RT, Hartree, Exc_Cor, Vloc (dt_evolve.f90:190-207)
         knew = kAc0 + Ac[it + 2][:, None]

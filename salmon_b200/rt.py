@@ -113,6 +113,14 @@ class GpuSystem:
         call("sgpu_update_vloc", self._h, None if r is None else _vp(r), _vp(e))
         return float(e[0]), float(e[1])
 
+    def vloc_history_reset(self):
+        """Vloc_old(:,1) = Vloc_old(:,2) = Vloc (control_sc.f90:82), for the etrs propagator."""
+        call("sgpu_vloc_history_reset", self._h)
+
+    def vloc_extrapolate(self):
+        """Vloc <- 3 Vloc - 3 Vloc_old(:,1) + Vloc_old(:,2), history shifted (dt_evolve.f90:248-252)."""
+        call("sgpu_vloc_extrapolate", self._h)
+
     def get_vloc(self):
         v = np.empty(self.sysm.NL)
         call("sgpu_get_vloc", self._h, _vp(v))

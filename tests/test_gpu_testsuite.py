@@ -76,6 +76,16 @@ def test_gs_eigenvalues_match_001(ground_state, tmp_path):
 def test_rt_current_and_energy_match_002(ground_state, precision, tmp_path):
     """002_bulk_rt starts from the orbital files 001 wrote: the ground state goes
     through gs_wfn_k/ (SALMON's unformatted layout) and is read back."""
+    _run_002(ground_state, precision, tmp_path, "middlepoint")
+
+
+def test_rt_etrs_matches_002(ground_state, tmp_path):
+    """The same run with propagator = 'etrs' (RT/dt_evolve.f90:218-348) in place
+    of the input's middle point: the table's rows hold within its tolerances."""
+    _run_002(ground_state, "c128", tmp_path, "etrs")
+
+
+def _run_002(ground_state, precision, tmp_path, propagator):
     from salmon_b200 import wfn_io
     from salmon_b200.rt import GpuSystem
     suite, sysm, kAc0, vpsl, esp, hist, zu_gs = ground_state
@@ -92,7 +102,7 @@ def test_rt_current_and_energy_match_002(ground_state, precision, tmp_path):
     with GpuSystem(sysm, precision) as g:
         g.set_state(zu)
         javt, energies = drive.rt_propagate(g, sysm, kAc0, vpsl, Ac, dt, nt + 1, energy_every=1, scf=True,
-                                            eion=eion)
+                                            eion=eion, propagator=propagator)
     # the rows as control_sc.f90 writes them: A and E = -dA/dt at step iter (transverse
     # geometry: total = external), J after step iter-1, and Eall_t(iter) = the energy
     # after step iter plus the field energy aLxyz |E|^2 / (8 pi)
@@ -101,4 +111,4 @@ def test_rt_current_and_energy_match_002(ground_state, precision, tmp_path):
     eall_t = {it: energies[it + 1] + sysm.aLxyz * float(E[it] @ E[it]) / (8 * np.pi) for it in range(nt + 1)}
     OUT.write_rt_data(str(tmp_path / "Si_rt.data"), dt, A, E, A, E, javt, nt)
     OUT.write_rt_energy_data(str(tmp_path / "Si_rt_energy.data"), dt, eall_t, energies[0], nt)
-    _check_table(suite["002_bulk_rt"], str(tmp_path), tag=precision + " ")
+    _check_table(suite["002_bulk_rt"], str(tmp_path), tag=f"{precision} {propagator} ")

@@ -63,3 +63,25 @@ def test_exact_scf_matches_001_eigenvalues():
         if r["file"] == "Si_eigen.data" and r["col"] == 2:
             ik, ib = divmod(r["row"], sysm.NB)
             assert abs(esp[ik, ib] - r["value"]) <= r["tol"], (r["label"], esp[ik, ib])
+
+
+def test_rt_oracle_propagators_converge_together():
+    """The CPU oracle's etrs and middle-point loops (oracle/rt_oracle.py) approach
+    each other as dt shrinks at a fixed final time.  Middle point takes the whole
+    step in the potential of the step's start (first order in the potential
+    coupling); etrs extrapolates it, so their difference falls at least
+    linearly with dt: about 2x per halving here."""
+    from oracle import rt_oracle as RO
+    from salmon_b200 import drive, system as S
+    sysm, kAc, vpsl, zu = S.small_system(8, 8, 12, nk=1, nb=2, seed=41)
+    kAc0 = np.ascontiguousarray(sysm.kAc0)
+    dz, dj = [], []
+    for nt in (16, 32):
+        dt = 0.32 / nt
+        Ac = drive.init_Ac(nt, dt, "impulse", epdir=(0.0, 0.0, 1.0), e_impulse=0.05)
+        z1, j1, _ = RO.rt_propagate(sysm, kAc0, vpsl, Ac, dt, nt, zu, "middlepoint")
+        z2, j2, _ = RO.rt_propagate(sysm, kAc0, vpsl, Ac, dt, nt, zu, "etrs")
+        dz.append(float(np.abs(z1 - z2).max()))
+        dj.append(float(np.abs(j1 - j2).max()))
+    assert dz[0] / dz[1] > 1.6 and dj[0] / dj[1] > 1.6, (dz, dj)
+    assert dz[1] < 2e-4
