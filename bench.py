@@ -535,20 +535,33 @@ def main():
             res[prec] = r
             g.close()
             continue
-        # end to end through the C ABI with host buffers: k+A(t) and V_loc in, rho and J out, every step
+        # end to end through the C ABI: k+A(t) and V_loc from host memory in, rho and J
+        # out to host memory, every step.  One rank: the host-result calls (the
+        # library stages through its own pinned buffers).  Several ranks: rho and J
+        # into device buffers, all-reduced on the device over NCCL (comm_summation
+        # of psi_rho.f90:88 and current.f90:286), then read back.
+        from salmon_b200 import dist as D
         kA = np.ascontiguousarray(kAc)
+        rho_d = torch.empty(NL, dtype=torch.float64, device="cuda")
+        jav_d = torch.empty(3, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
         e0.record(stream)
         for it in range(args.steps):
             kt = kA + np.array([0.0, 0.0, 1e-4 * it])[:, None]
             g.update_projector(kt)
             g.set_vloc(vloc)
             g.hamiltonian(DT, flag_current=True)  # the current's stencil sums with the step
-            rho = g.psi_rho_RT()
-            jav = g.current_RT(kt)
-            if world > 1:  # comm_summation of rho and J (psi_rho.f90:88, current.f90:286) over NCCL
-                from salmon_b200 import dist as D
-                rho = D.comm_summation(rho)
-                jav = D.comm_summation(jav)
+            if world == 1:
+                rho = g.psi_rho_RT()
+                jav = g.current_RT(kt)
+            else:
+                g.psi_rho_dev(rho_d.data_ptr())
+                g.current_dev(kt, jav_d.data_ptr())
+                D.comm_summation_dev(g, rho_d)
+                D.comm_summation_dev(g, jav_d)
+                with torch.cuda.stream(stream):
+                    rho = rho_d.cpu().numpy()
+                    jav = jav_d.cpu().numpy()
         e1.record(stream)
         e1.synchronize()
         ms_e2e = max_over_ranks(e0.elapsed_time(e1))

@@ -219,6 +219,24 @@ module salmon_gpu
       import :: c_int, c_ptr
       type(c_ptr), value :: h
     end function
+    integer(c_int) function sgpu_check_desc(desc) bind(C, name="sgpu_check_desc")
+      import :: c_int, sgpu_desc
+      type(sgpu_desc), intent(in) :: desc
+    end function
+    ! device outputs for an allreduce on the device (psi_rho.f90:88, current.f90:286)
+    integer(c_int) function sgpu_psi_rho_dev(h, rho_dev) bind(C, name="sgpu_psi_rho_dev")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h, rho_dev
+    end function
+    integer(c_int) function sgpu_current_dev(h, kac, jav_dev) bind(C, name="sgpu_current_dev")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h, jav_dev
+      real(c_double), intent(in) :: kac(*)
+    end function
+    integer(c_int) function sgpu_update_vloc_dev(h, rho_dev, eh_exc_dev) bind(C, name="sgpu_update_vloc_dev")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h, rho_dev, eh_exc_dev
+    end function
     integer(c_int) function sgpu_batch_create(handles, n, b) bind(C, name="sgpu_batch_create")
       import :: c_int, c_ptr
       type(c_ptr), intent(in) :: handles(*)

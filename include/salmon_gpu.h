@@ -95,6 +95,13 @@ typedef struct sgpu_system* sgpu_handle;
 
 /* ---- lifetime ------------------------------------------------------------ */
 
+/* The argument checks sgpu_create runs on a descriptor (sizes, the k range,
+ * the projector tables' index ranges), on the host only: no device call, so a
+ * rank can validate its k-block's descriptor before it touches a GPU.  0 or
+ * SGPU_ERR_ARG / SGPU_ERR_UNSUPPORTED with the reason in sgpu_last_error.
+ * No reference counterpart (the reference checks its input in read_input). */
+int sgpu_check_desc(const sgpu_desc* desc);
+
 /* Builds the device copies of every table in *desc on the current CUDA device
  * and allocates the resident orbital array and Taylor workspace.
  * Replaces: opt_vars_initialize_p2 + init_projector
@@ -154,6 +161,11 @@ int sgpu_set_vpsl(sgpu_handle h, const double* vpsl);
  * may be NULL) receives the Hartree energy 1/2 sum Vh rho Hxyz and the
  * exchange-correlation energy sum exc rho Hxyz.  Grid sizes must be 2^a 3^b <= 96. */
 int sgpu_update_vloc(sgpu_handle h, const double* rho, double* eh_exc);
+
+/* sgpu_update_vloc from a DEV density rho_dev(NL) (e.g. after an allreduce on
+ * the device), enqueued on the handle's stream and not waited for; eh_exc_dev
+ * (DEV [2], may be NULL) receives the Hartree and XC energies. */
+int sgpu_update_vloc_dev(sgpu_handle h, const double* rho_dev, double* eh_exc_dev);
 
 /* device -> HOST Vloc(NL) (FP64). */
 int sgpu_get_vloc(sgpu_handle h, double* vloc);
@@ -239,11 +251,21 @@ int sgpu_psi_rho(sgpu_handle h, double* rho_l);
 int sgpu_psi_rho_static(int precision, int NL, int nb, int nk, const void* zu, const double* occ, int ld_occ,
                         double* rho, void* stream);
 
+/* The same density into a DEV array rho_dev(NL) of the handle's device,
+ * enqueued on the handle's stream and not waited for: the per-rank density
+ * that psi_rho.f90:88 allreduces, left on the device for a collective
+ * (ncclAllReduce on the handle's stream) and sgpu_update_vloc_dev. */
+int sgpu_psi_rho_dev(sgpu_handle h, double* rho_dev);
+
 /* Macroscopic current of the resident orbitals at k+A = kAc (HOST (NK,3));
  * jav(3) HOST, before the allreduce.  Rebuilds the projectors for kAc, as
  * current() does.  Replaces current('RT',...) impl
  * (RT/current.f90:78-292, current_stencil stencil/F90/current.f90:16-115). */
 int sgpu_current(sgpu_handle h, const double* kAc, double* jav);
+
+/* The same current into DEV jav_dev[3], enqueued on the handle's stream and
+ * not waited for (the per-rank value that current.f90:286 allreduces). */
+int sgpu_current_dev(sgpu_handle h, const double* kAc, double* jav_dev);
 
 /* Kinetic and nonlocal energies of the resident orbitals at kAc (HOST):
  *   Ekin = sum occ (Hxyz <psi|T + kAc.nabla|psi> + |kAc|^2/2),

@@ -60,6 +60,10 @@ ABI = {
     "sgpu_autotune": (C.c_int, [_vp, _ip, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]),
     "sgpu_vloc_history_reset": (C.c_int, [_vp]),
     "sgpu_vloc_extrapolate": (C.c_int, [_vp]),
+    "sgpu_check_desc": (C.c_int, [_vp]),
+    "sgpu_psi_rho_dev": (C.c_int, [_vp, _vp]),
+    "sgpu_current_dev": (C.c_int, [_vp, _vp, _vp]),
+    "sgpu_update_vloc_dev": (C.c_int, [_vp, _vp, _vp]),
     "sgpu_batch_create": (C.c_int, [C.POINTER(C.c_void_p), _ip, C.POINTER(C.c_void_p)]),
     "sgpu_batch_step": (C.c_int, [_vp, _vp, _ip]),
     "sgpu_batch_stream": (C.c_void_p, [_vp]),

@@ -185,11 +185,43 @@ extern "C" {
 
 const char* sgpu_last_error(void) { return g_err.c_str(); }
 
+int sgpu_check_desc(const sgpu_desc* d) {
+  if (!d) return fail(SGPU_ERR_ARG, "sgpu_check_desc: null descriptor");
+  if (d->NLx < 1 || d->NLy < 1 || d->NLz < 1) return fail(SGPU_ERR_ARG, "sgpu_create: grid sizes must be positive");
+  if (d->NK < 1 || d->NK_s < 1 || d->NK_e < d->NK_s || d->NK_e > d->NK)
+    return fail(SGPU_ERR_ARG, "sgpu_create: need 1 <= NK_s <= NK_e <= NK");
+  if (d->NB < 1 || d->NBoccmax < 1 || d->NBoccmax > d->NB)
+    return fail(SGPU_ERR_ARG, "sgpu_create: need 1 <= NBoccmax <= NB");
+  if (d->NI < 0 || d->Nlma < 0 || d->Nps < 0 || (d->NI > 0 && d->Nlma > 0 && d->Nps < 1))
+    return fail(SGPU_ERR_ARG, "sgpu_create: bad NI/Nps/Nlma");
+  if (!d->occ) return fail(SGPU_ERR_ARG, "sgpu_create: occ is NULL");
+  if (d->Nlma > 0 && (!d->Mps || !d->Jxyz || !d->Jxx || !d->Jyy || !d->Jzz || !d->uV || !d->iuV || !d->a_tbl))
+    return fail(SGPU_ERR_ARG, "sgpu_create: projector tables missing");
+  if ((d->NLz % 2 == 0 ? d->NLz / 2 : d->NLz) > 128)
+    return fail(SGPU_ERR_UNSUPPORTED, "sgpu_create: NLz too large for the stencil pass");
+  const long NL = (long)d->NLx * d->NLy * d->NLz;
+  if (NL > (1L << 30)) return fail(SGPU_ERR_ARG, "sgpu_create: grid too large");
+  if (d->Nlma > 0) {
+    for (int a = 0; a < d->NI; ++a) {
+      const int m = d->Mps[a];
+      if (m < 0 || m > d->Nps) return fail(SGPU_ERR_ARG, "sgpu_create: Mps out of range");
+      for (int j = 0; j < m; ++j) {
+        const long gi = (long)d->Jxyz[(size_t)a * d->Nps + j] - 1;
+        if (gi < 0 || gi >= NL) return fail(SGPU_ERR_ARG, "sgpu_create: Jxyz out of range");
+      }
+    }
+    for (int l = 0; l < d->Nlma; ++l)
+      if (d->a_tbl[l] < 1 || d->a_tbl[l] > d->NI) return fail(SGPU_ERR_ARG, "sgpu_create: a_tbl out of range");
+  }
+  return 0;
+}
+
 int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
   if (!d || !out) return fail(SGPU_ERR_ARG, "sgpu_create: null argument");
   *out = nullptr;
   if (precision != SGPU_PREC_C128 && precision != SGPU_PREC_C64)
     return fail(SGPU_ERR_ARG, "sgpu_create: precision must be SGPU_PREC_C128 or SGPU_PREC_C64");
+  if (int rc = sgpu_check_desc(d)) return rc;
   if (d->NLx < 1 || d->NLy < 1 || d->NLz < 1) return fail(SGPU_ERR_ARG, "sgpu_create: grid sizes must be positive");
   if (d->NK < 1 || d->NK_s < 1 || d->NK_e < d->NK_s || d->NK_e > d->NK)
     return fail(SGPU_ERR_ARG, "sgpu_create: need 1 <= NK_s <= NK_e <= NK");
@@ -639,6 +671,24 @@ int sgpu_psi_rho(sgpu_handle h, double* rho_l) {
   return 0;
 }
 
+int sgpu_psi_rho_dev(sgpu_handle h, double* rho_dev) {
+  if (!valid(h) || !rho_dev) return fail(SGPU_ERR_ARG, "sgpu_psi_rho_dev: null argument");
+  System* s = h;
+  if (!s->have_state) return fail(SGPU_ERR_STATE, "sgpu_psi_rho_dev: no state loaded");
+  CK(sgpu::launch_psi_rho(*s, rho_dev));
+  return 0;
+}
+
+int sgpu_current_dev(sgpu_handle h, const double* kAc, double* jav_dev) {
+  if (!valid(h) || !kAc || !jav_dev) return fail(SGPU_ERR_ARG, "sgpu_current_dev: null argument");
+  System* s = h;
+  if (!s->have_state) return fail(SGPU_ERR_STATE, "sgpu_current_dev: no state loaded");
+  int rc = sgpu_update_projector(h, kAc);  // current() rebuilds the projectors (current.f90:125)
+  if (rc) return rc;
+  CK(sgpu::launch_current(*s, jav_dev));
+  return 0;
+}
+
 int sgpu_current(sgpu_handle h, const double* kAc, double* jav) {
   if (!valid(h) || !kAc || !jav) return fail(SGPU_ERR_ARG, "sgpu_current: null argument");
   System* s = h;
@@ -894,6 +944,17 @@ int sgpu_update_vloc(sgpu_handle h, const double* rho, double* eh_exc) {
   CK(sgpu::launch_update_vloc(*s, s->rho_d, s->exc_d));
   if (eh_exc) CK(cudaMemcpyAsync(eh_exc, s->exc_d, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
+  s->have_vloc = true;
+  return 0;
+}
+
+int sgpu_update_vloc_dev(sgpu_handle h, const double* rho_dev, double* eh_exc_dev) {
+  if (!valid(h) || !rho_dev) return fail(SGPU_ERR_ARG, "sgpu_update_vloc_dev: null argument");
+  System* s = h;
+  if (!s->vpsl) return fail(SGPU_ERR_STATE, "sgpu_update_vloc_dev: call sgpu_set_vpsl first");
+  if (!(sgpu::fft_size_ok(s->NLx) && sgpu::fft_size_ok(s->NLy) && sgpu::fft_size_ok(s->NLz)))
+    return fail(SGPU_ERR_UNSUPPORTED, "sgpu_update_vloc_dev: grid sizes must be 2^a 3^b <= 96");
+  CK(sgpu::launch_update_vloc(*s, rho_dev, eh_exc_dev ? eh_exc_dev : s->exc_d));
   s->have_vloc = true;
   return 0;
 }

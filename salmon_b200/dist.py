@@ -5,7 +5,10 @@ The reference distributes k-points over the ranks of nproc_group_tdks
 with comm_summation (common/psi_rho.f90:88, RT/current.f90:286); every rank
 keeps the whole grid.  Here each rank holds one handle for its k-block; the
 Taylor step has no exchange, and rho / J are reduced once per step over
-torch.distributed (NCCL over NVLink on GPUs, gloo on CPU for the tests).
+torch.distributed (NCCL over NVLink on GPUs, gloo on CPU for the tests):
+comm_summation for host values, comm_summation_dev for device buffers that
+the library filled (sgpu_psi_rho_dev, sgpu_current_dev), reduced in place on
+the library's stream with no host round trip.
 """
 from __future__ import annotations
 
@@ -53,3 +56,29 @@ def comm_summation(x, group=None):
     dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
     out = t.cpu().numpy()
     return out if np.ndim(x) else float(out)
+
+
+def comm_summation_dev(g, t, group=None):
+    """In-place allreduce-sum of the CUDA tensor t over the default process group,
+    ordered on the stream of the GpuSystem g: after the kernels that filled t
+    (sgpu_psi_rho_dev / sgpu_current_dev on g.stream) and before the handle's
+    next work (e.g. sgpu_update_vloc_dev reading t).  No host copy."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return t
+    with torch.cuda.stream(torch.cuda.ExternalStream(g.stream)):
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return t
+
+
+def local_descriptors_valid(sysm, world: int):
+    """Every rank's k-block descriptor passes the library's host-side checks
+    (sgpu_check_desc; no device needed).  Returns the (NK_s, NK_e) blocks."""
+    from .rt import check_desc
+    blocks = []
+    for r in range(world):
+        loc = local_system(sysm, r, world)
+        check_desc(loc)
+        blocks.append((loc.NK_s, loc.NK_e))
+    return blocks

@@ -267,6 +267,20 @@ class GpuSystem:
         call("sgpu_psi_rho", self._h, _vp(rho))
         return rho
 
+    def psi_rho_dev(self, rho_dev: int):
+        """rho(NL) of the resident orbitals into the DEV FP64 buffer at rho_dev,
+        enqueued on the handle's stream (not waited for)."""
+        call("sgpu_psi_rho_dev", self._h, C.c_void_p(rho_dev))
+
+    def current_dev(self, kAc, jav_dev: int):
+        """J(3) at kAc into the DEV FP64 buffer at jav_dev, on the handle's stream."""
+        k = np.ascontiguousarray(np.asarray(kAc, dtype=np.float64))
+        call("sgpu_current_dev", self._h, _vp(k), C.c_void_p(jav_dev))
+
+    def update_vloc_dev(self, rho_dev: int, eh_exc_dev: int = 0):
+        """Vloc = Vh + Vpsl + Vexc from the DEV density at rho_dev, on the handle's stream."""
+        call("sgpu_update_vloc_dev", self._h, C.c_void_p(rho_dev), C.c_void_p(eh_exc_dev or None))
+
     def current_RT(self, kAc):
         k = np.ascontiguousarray(kAc, dtype=np.float64)
         jav = np.empty(3)
@@ -278,6 +292,13 @@ class GpuSystem:
         ek, en = C.c_double(), C.c_double()
         call("sgpu_energy_terms", self._h, _vp(k), C.byref(ek), C.byref(en))
         return ek.value, en.value
+
+
+def check_desc(sysm) -> None:
+    """The descriptor checks of sgpu_create on the host (no device call);
+    raises SalmonGPUError with the library's reason."""
+    d = sysm.desc()
+    call("sgpu_check_desc", C.byref(d))
 
 
 class GpuBatch:
@@ -310,4 +331,4 @@ class GpuBatch:
         self.close()
 
 
-__all__ = ["GpuSystem", "GpuBatch", "SalmonGPUError", "PRECISIONS"]
+__all__ = ["GpuSystem", "GpuBatch", "SalmonGPUError", "PRECISIONS", "check_desc"]

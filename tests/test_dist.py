@@ -1,6 +1,8 @@
 """k-point sharding host logic with world_size 2 over gloo on CPU: each rank
-computes rho, J and the energy terms of its k-block with the CPU oracle and the
-sums over ranks equal the single-process results (1e-12)."""
+builds its k-block's descriptor and has the library check it on the host
+(sgpu_check_desc, no device), computes rho, J and the energy terms of its block
+with the CPU oracle, and the sums over ranks equal the single-process results
+(1e-12)."""
 import os
 import socket
 
@@ -35,8 +37,20 @@ def _worker(rank, world, port, out_dir):
     try:
         from oracle import oracle as O
         from salmon_b200 import system as S
+        from salmon_b200.rt import SalmonGPUError, check_desc
         sysm, kAc, vloc, zu = S.small_system(8, 8, 10, nk=3, nb=4)
         loc = D.local_system(sysm, rank, world)
+        # the library's host-side checks of this rank's descriptor (no device call)
+        check_desc(loc)
+        d = loc.desc()
+        assert (d.NK, d.NK_s, d.NK_e) == (sysm.NK,) + D.k_range(sysm.NK, world, rank)
+        bad = D.local_system(sysm, rank, world)
+        bad.NK_e = sysm.NK + 1
+        try:
+            check_desc(bad)
+            raise AssertionError("a k range beyond NK was accepted")
+        except SalmonGPUError:
+            pass
         zl = D.local_orbitals(zu, loc)
         rho = D.comm_summation(O.psi_rho(loc, zl))
         jav = D.comm_summation(O.current(loc, kAc, zl))
@@ -63,3 +77,11 @@ def test_sharded_reductions_equal_single_process(tmp_path):
         np.testing.assert_allclose(r["rho"], rho0, rtol=1e-12, atol=1e-14)
         np.testing.assert_allclose(r["jav"], j0, rtol=1e-12, atol=1e-16)
         np.testing.assert_allclose(r["e"], e0, rtol=1e-12)
+
+
+def test_every_rank_descriptor_passes_the_library_checks():
+    from salmon_b200 import system as S
+    sysm, kAc, vloc, zu = S.microbench_system(16, nkgrid=(4, 4, 4), Nb=8, with_orbitals=False)
+    for world in (1, 2, 3, 8):
+        blocks = D.local_descriptors_valid(sysm, world)
+        assert blocks == [D.k_range(sysm.NK, world, r) for r in range(world)]
