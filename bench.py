@@ -227,7 +227,7 @@ def batched_bench(nsteps=1000, per_replay=10):
     graph replays of `per_replay` Taylor steps; beside it the same systems stepped
     one sgpu_hamiltonian call at a time."""
     import torch
-    from salmon_b200 import system as S
+    from salmon_b200 import system as S, tune
     from salmon_b200.rt import GpuBatch, GpuSystem
     gs, tuned, norb = [], {}, 0
     for name, (cells, grid, nkg, nb) in S.BATCHED_SYSTEMS.items():
@@ -236,9 +236,8 @@ def batched_bench(nsteps=1000, per_replay=10):
         g.set_state(zu)
         g.set_vloc(vloc)
         g.update_projector(kAc)
-        ns, sp, ms = g.autotune(reps=3)
-        tuned[name] = {"nslab": ns, "uvpsi_split": sp, "ms_per_h_apply": ms, "norb": sysm.nk_local * nb,
-                       "grid": list(grid)}
+        entry, source = tune.apply(g, sysm, "c64", write=False)  # the launch-shape table (tuned if absent)
+        tuned[name] = {"params": entry["params"], "from": source, "norb": sysm.nk_local * nb, "grid": list(grid)}
         norb += sysm.nk_local * nb
         gs.append(g)
     dts = [DT] * len(gs)
@@ -284,7 +283,7 @@ def large_bench(nsteps=10):
     orbitals made on the device; Taylor-step throughput in complex(4) (launch
     shapes autotuned) and complex(8)."""
     import torch
-    from salmon_b200 import system as S
+    from salmon_b200 import system as S, tune
     from salmon_b200.rt import GpuSystem
     sysm, kAc, vloc, _ = S.si_supercell_system((3, 3, 3), (48, 48, 48), (2, 2, 1), 432, with_orbitals=False)
     norb = sysm.nk_local * sysm.NBoccmax
@@ -297,7 +296,7 @@ def large_bench(nsteps=10):
         g.set_state_dev(z.data_ptr())
         g.set_vloc(vloc)
         g.update_projector(kAc)
-        tuned = g.autotune(reps=2) if prec == "c64" else None
+        tuned = tune.apply(g, sysm, prec, write=False)
         st = torch.cuda.ExternalStream(g.stream)
         for _ in range(2):
             g.hamiltonian(DT)
@@ -312,8 +311,7 @@ def large_bench(nsteps=10):
         ms = e0.elapsed_time(e1) / nsteps
         out[prec] = {"ms_per_step": ms, "orbital_updates_per_s": norb / (ms * 1e-3),
                      "stencil_pass_ms": g.time_kernel("stencil_pass", reps=3)}
-        if tuned:
-            out[prec]["tuned"] = {"nslab": tuned[0], "uvpsi_split": tuned[1]}
+        out[prec]["tuned"] = {"params": tuned[0]["params"], "from": tuned[1]}
         g.close()
     del z
     out["fp32_over_fp64"] = out["c64"]["orbital_updates_per_s"] / out["c128"]["orbital_updates_per_s"]

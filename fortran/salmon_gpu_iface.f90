@@ -237,6 +237,14 @@ module salmon_gpu
       import :: c_int, c_ptr
       type(c_ptr), value :: h, rho_dev, eh_exc_dev
     end function
+    integer(c_int) function sgpu_autotune_step(h, dt, reps, params, ms) bind(C, name="sgpu_autotune_step")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h
+      real(c_double), value :: dt
+      integer(c_int), value :: reps
+      integer(c_int), intent(out) :: params(6)
+      real(c_double), intent(out) :: ms
+    end function
     integer(c_int) function sgpu_batch_create(handles, n, b) bind(C, name="sgpu_batch_create")
       import :: c_int, c_ptr
       type(c_ptr), intent(in) :: handles(*)

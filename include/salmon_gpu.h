@@ -334,11 +334,13 @@ enum {
   SGPU_PARAM_CUR_FIXED = 7,   /* current and energy stencils: 1 splits each 32x32 plane over four
                                  CTAs (48x48: six), 2 32x32 planes of the current over two, 0 the
                                  generic kernels                                                     */
-  SGPU_PARAM_TAYLOR_KERNEL = 8 /* Taylor step: 1 four stencil passes over all orbitals (any grid), 2
+  SGPU_PARAM_TAYLOR_KERNEL = 8, /* Taylor step: 1 four stencil passes over all orbitals (any grid), 2
                                  the orbitals of a band group resident in one CTA's shared memory for
                                  the whole step (16x16, 16x32 and 20x20 planes where they fit), 0 the
                                  resident form where it is the faster one (complex(4), 16x16 planes),
                                  else the passes                                                     */
+  SGPU_PARAM_NSP = 9          /* sphere points of the handle (read only): the union of the
+                                 projectors' points, a key of the launch-shape table              */
 };
 
 /* CG preconditioners.  PLAIN is the reference's CG_ompk.  TPA multiplies the
@@ -364,6 +366,20 @@ int sgpu_get_param(sgpu_handle h, int param, int* value);
  * modified.  No reference counterpart; the nearest is auto_blocking
  * (modules/opt_variables.f90:340-353). */
 int sgpu_autotune(sgpu_handle h, int reps, int* nslab, int* split, double* ms_per_apply);
+
+/* Step tuner: times whole Taylor steps of length dt (reps per candidate, after a
+ * warm-up) on a copy of the resident orbitals, for every launch choice that
+ * applies to the handle's grid and precision: the Taylor form
+ * (SGPU_PARAM_TAYLOR_KERNEL 2 where the resident form fits, else 1), and for
+ * the stencil passes the compile-time plane shapes (SGPU_PARAM_PASS_FIXED),
+ * the table staging (SGPU_PARAM_PASS_TABLES), x-slabs (SGPU_PARAM_NSLAB 1, 2,
+ * 4) and the KB kernel (tile, or band quad with split 1, 2, 4, 8).  Keeps the
+ * fastest in the handle.  params (HOST [6], may be NULL) receives
+ * {taylor_kernel, pass_fixed, pass_tables, nslab, kb_kernel, uvpsi_split};
+ * ms_per_step (may be NULL) its time.  The resident orbitals are not modified.
+ * No reference counterpart; the nearest is auto_blocking
+ * (modules/opt_variables.f90:340-353). */
+int sgpu_autotune_step(sgpu_handle h, double dt, int reps, int* params, double* ms_per_step);
 
 /* ---- CG preconditioners (ground state) ------------------------------------ */
 /* The TPA preconditioner applied to nvec DEV complex(8) vectors (layout

@@ -64,6 +64,7 @@ ABI = {
     "sgpu_psi_rho_dev": (C.c_int, [_vp, _vp]),
     "sgpu_current_dev": (C.c_int, [_vp, _vp, _vp]),
     "sgpu_update_vloc_dev": (C.c_int, [_vp, _vp, _vp]),
+    "sgpu_autotune_step": (C.c_int, [_vp, C.c_double, _ip, C.POINTER(C.c_int), _dp]),
     "sgpu_batch_create": (C.c_int, [C.POINTER(C.c_void_p), _ip, C.POINTER(C.c_void_p)]),
     "sgpu_batch_step": (C.c_int, [_vp, _vp, _ip]),
     "sgpu_batch_stream": (C.c_void_p, [_vp]),
@@ -71,7 +72,7 @@ ABI = {
 }
 
 PARAMS = {"nslab": 0, "launches": 1, "uvpsi_split": 2, "cg_precond": 3, "pass_tables": 4, "kb_kernel": 5,
-          "pass_fixed": 6, "cur_fixed": 7, "taylor_kernel": 8}
+          "pass_fixed": 6, "cur_fixed": 7, "taylor_kernel": 8, "nsp": 9}
 
 KERNELS = {"stencil_pass": 0, "taylor_stage": 1, "taylor_last": 1, "uvpsi": 2, "psi_rho": 3, "kb_field": 4, "kb_term": 5}
 

@@ -140,12 +140,19 @@ void sgpu::taylor_stage_coefs(double dt, double c[4][2]) {
 // (kernel launches only, so it can be captured into a CUDA graph): four stages
 // zu -> tw0 -> tw1 -> tw0 -> zu.
 cudaError_t sgpu::enqueue_taylor_step(System& sys, double dt, bool gather_first, bool with_current) {
+  return enqueue_taylor_step_on(sys, sys.zu, dt, gather_first, with_current);
+}
+
+// The same step on the orbital array zu_buf (s->zu, or a copy the tuner times:
+// tw[2], with tw[0] and tw[1] as the stages' workspace).
+cudaError_t sgpu::enqueue_taylor_step_on(System& sys, void* zu_buf, double dt, bool gather_first,
+                                         bool with_current) {
   System* s = &sys;
   s->cur_valid = false;
   const bool resident = s->taylor_kernel == 2 || (s->taylor_kernel == 0 && sgpu::resident_step_default(*s));
   if (resident) {
     // the whole step on chip, a band group per CTA (it gathers its own projections)
-    cudaError_t e = sgpu::launch_taylor_resident(*s, s->zu, dt, with_current ? s->cur_part : nullptr,
+    cudaError_t e = sgpu::launch_taylor_resident(*s, zu_buf, dt, with_current ? s->cur_part : nullptr,
                                                  s->nsp > 0 ? s->Sbuf : nullptr);
     if (e != cudaSuccess) return e;
     s->S_valid = s->nsp > 0;
@@ -157,8 +164,8 @@ cudaError_t sgpu::enqueue_taylor_step(System& sys, double dt, bool gather_first,
   taylor_stage_coefs(dt, c);
   // Each stage exports its output at the sphere points (S); the next stage's
   // projections read S instead of gathering from the full orbitals.
-  const void* ins[4] = {s->zu, s->tw[0], s->tw[1], s->tw[0]};
-  void* outs[4] = {s->tw[0], s->tw[1], s->tw[0], s->zu};
+  const void* ins[4] = {zu_buf, s->tw[0], s->tw[1], s->tw[0]};
+  void* outs[4] = {s->tw[0], s->tw[1], s->tw[0], zu_buf};
   cudaError_t e;
   for (int n = 0; n < 4; ++n) {
     sgpu::PassIO io;
@@ -172,7 +179,7 @@ cudaError_t sgpu::enqueue_taylor_step(System& sys, double dt, bool gather_first,
     if (e != cudaSuccess) return e;
   }
   s->S_valid = s->nsp > 0;
-  if (with_current) {  // the stencil sums of the new orbitals, right after the update
+  if (with_current && zu_buf == s->zu) {  // the stencil sums of the new orbitals, right after the update
     int nx = 1;
     if ((e = sgpu::launch_current_stencil(*s, s->cur_part, nx)) != cudaSuccess) return e;
     s->cur_nx = nx;
@@ -1098,6 +1105,7 @@ extern "C" int sgpu_get_param(sgpu_handle h, int param, int* value) {
     case SGPU_PARAM_PASS_FIXED: *value = h->pass_fixed; return 0;
     case SGPU_PARAM_CUR_FIXED: *value = h->cur_fixed; return 0;
     case SGPU_PARAM_TAYLOR_KERNEL: *value = h->taylor_kernel; return 0;
+    case SGPU_PARAM_NSP: *value = h->nsp; return 0;
     default: return fail(SGPU_ERR_ARG, "sgpu_get_param: unknown parameter");
   }
 }
@@ -1155,5 +1163,73 @@ extern "C" int sgpu_autotune(sgpu_handle h, int reps, int* nslab, int* split, do
   if (nslab) *nslab = bs;
   if (split) *split = bk;
   if (ms) *ms = best;
+  return 0;
+}
+
+// ------------------------------------------------------------ step tuner --
+// Times whole Taylor steps on a copy of the orbitals (tw[2]; the resident
+// orbitals are not modified) for every combination of the launch choices that
+// apply to the handle's shapes, keeps the fastest in the handle and returns it.
+extern "C" int sgpu_autotune_step(sgpu_handle h, double dt, int reps, int* params, double* ms_per_step) {
+  if (!valid(h) || reps < 1) return fail(SGPU_ERR_ARG, "sgpu_autotune_step: bad argument");
+  System* s = h;
+  if (!s->have_state || !s->have_vloc || !s->have_proj)
+    return fail(SGPU_ERR_STATE, "sgpu_autotune_step: state, Vloc and projectors must be set first");
+  const size_t bytes = (size_t)s->norb * s->NL * s->elem;
+  CK(cudaMemcpyAsync(s->tw[2], s->zu, bytes, cudaMemcpyDeviceToDevice, s->stream));
+  const int old[6] = {s->taylor_kernel, s->pass_fixed, s->pass_tab, s->nslab, s->kb_kernel, s->um_split};
+  auto apply = [&](const int* p) {
+    s->taylor_kernel = p[0]; s->pass_fixed = p[1]; s->pass_tab = p[2]; s->nslab = p[3]; s->kb_kernel = p[4];
+    s->um_split = p[5];
+  };
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  double best = 1e300;
+  int bp[6] = {old[0], old[1], old[2], old[3], old[4], old[5]};
+  cudaError_t err = cudaSuccess;
+  std::vector<std::array<int, 6>> cands;
+  if (sgpu::resident_step_fits(*s)) cands.push_back({2, old[1], old[2], old[3], old[4], old[5]});
+  for (int pf : {1, 0})
+    for (int pt : {1, 0})
+      for (int ns : {1, 2, 4}) {
+        if (ns > 1 && s->NLx / ns < 8) continue;
+        for (int sp : {0, 1, 2, 4, 8}) {  // 0: the band-group tile kernel
+          if (sp == 0 && !sgpu::kb_tile_fits(*s)) continue;
+          cands.push_back({1, pf, pt, ns, sp ? 2 : 1, sp ? sp : old[5]});
+        }
+      }
+  for (const auto& c : cands) {
+    apply(c.data());
+    if ((err = sgpu::prepare_pass(*s)) != cudaSuccess) break;
+    if ((err = sgpu::prepare_resident(*s)) != cudaSuccess) break;
+    err = sgpu::enqueue_taylor_step_on(*s, s->tw[2], dt, true, false);  // warm-up
+    if (err == cudaSuccess) err = cudaEventRecord(e0, s->stream);
+    for (int r = 0; r < reps && err == cudaSuccess; ++r)
+      err = sgpu::enqueue_taylor_step_on(*s, s->tw[2], dt, r == 0, false);
+    if (err == cudaSuccess) err = cudaEventRecord(e1, s->stream);
+    if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+    float t = 0;
+    if (err == cudaSuccess) err = cudaEventElapsedTime(&t, e0, e1);
+    if (err != cudaSuccess) break;
+    if (t / reps < best) {
+      best = t / reps;
+      for (int k = 0; k < 6; ++k) bp[k] = c[k];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  s->S_valid = false;  // the timed steps overwrote S
+  s->cur_valid = false;
+  if (err != cudaSuccess) {
+    apply(old);
+    return cuda_fail(err, "sgpu_autotune_step");
+  }
+  apply(bp);
+  if (sgpu::prepare_pass(*s) != cudaSuccess || sgpu::prepare_resident(*s) != cudaSuccess)
+    return fail(SGPU_ERR_CUDA, "sgpu_autotune_step: setup of the chosen shapes failed");
+  if (params)
+    for (int k = 0; k < 6; ++k) params[k] = bp[k];
+  if (ms_per_step) *ms_per_step = best;
   return 0;
 }

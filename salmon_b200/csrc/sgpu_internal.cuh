@@ -331,6 +331,7 @@ void set_last_error(const std::string& msg);
 // with_current: also compute the current's stencil sums of the new orbitals
 // into cur_part (flag_current of RT/hamiltonian.f90:27).
 cudaError_t enqueue_taylor_step(System& s, double dt, bool gather_first, bool with_current = false);
+cudaError_t enqueue_taylor_step_on(System& s, void* zu_buf, double dt, bool gather_first, bool with_current);
 
 // The Taylor step with each orbital resident in one CTA's shared memory
 // (k_resident.cu): whether the handle's grid and precision have that form, the

@@ -166,6 +166,22 @@ class GpuSystem:
         call("sgpu_autotune", self._h, int(reps), C.byref(ns), C.byref(sp), C.byref(ms))
         return ns.value, sp.value, ms.value
 
+    TUNE_PARAMS = ("taylor_kernel", "pass_fixed", "pass_tables", "nslab", "kb_kernel", "uvpsi_split")
+
+    def autotune_step(self, dt: float = 0.02, reps: int = 3):
+        """Times whole Taylor steps for every launch choice (sgpu_autotune_step),
+        keeps the fastest; returns ({param: value}, ms per step)."""
+        p = (C.c_int * 6)()
+        ms = C.c_double()
+        call("sgpu_autotune_step", self._h, C.c_double(dt), int(reps), p, C.byref(ms))
+        return dict(zip(self.TUNE_PARAMS, list(p))), ms.value
+
+    def get_nsp(self) -> int:
+        """Sphere points of the handle (the union of the projectors' points)."""
+        v = C.c_int()
+        call("sgpu_get_param", self._h, _lib.PARAMS["nsp"], C.byref(v))
+        return v.value
+
     def time_kernel(self, kernel: str, reps: int = 10) -> float:
         """Mean device milliseconds per launch of one library kernel (CUDA events on the library stream)."""
         ms = C.c_double()
