@@ -325,7 +325,6 @@ def precond_bench(max_outer=60):
     pairs from plain CG on one displaced configuration (sigma = 0.05 bohr),
     evaluated on another, against TPA alone and plain CG (capped at
     `max_outer` iterations)."""
-    from oracle import net_oracle as N   # the identity weights the network starts from
     from salmon_b200 import precond as P
     from salmon_b200.rt import GpuSystem
     base = dict(ncell=(2, 2, 2), grid=(32, 32, 32), nkgrid=(2, 2, 2), Nb=144, Nocc=128)
@@ -342,9 +341,11 @@ def precond_bench(max_outer=60):
     t0 = time.perf_counter()
     sysm, g = gpu(101)
     R, E, kidx, tb = P.cg_training_pairs(g, sysm, 128, snap_at=(10, 20, 40), bands=(0, 31, 63, 95, 127))
-    g.net_set_weights(N.identity_weights(noise=1e-2, seed=0))
-    hist = P.train(g, P.tpa_inputs(g, R, kidx, tb), E, steps=400, batch=16, lr=2e-3)
-    w = g.net_get_weights()
+    vsys, gv = gpu(303)  # held-out validation configuration
+    zv = gv.gs_get_state()
+    w, report, chosen = P.train_and_select(g, P.tpa_inputs(g, R, kidx, tb), E, P.DEFAULT_VARIANTS,
+                                           lambda wt: P.cg_cost(gv, zv, wt, max_outer=max_outer, nconv=128))
+    gv.close()
     g.close()
     t_train = time.perf_counter() - t0
     runs = {}
@@ -364,7 +365,7 @@ def precond_bench(max_outer=60):
     return {"runs": runs, "learned_vs_plain_iterations": runs["learned"]["cg_iterations"] / runs["plain"]["cg_iterations"],
             "learned_vs_tpa_iterations": runs["learned"]["cg_iterations"] / runs["tpa"]["cg_iterations"],
             "eigenvalue_max_abs_diff_learned_vs_tpa": de, "training_pairs": int(R.shape[0]),
-            "training_loss": [float(np.mean(hist[:5])), float(np.mean(hist[-20:]))], "training_seconds": t_train,
+            "selection": {k: list(v) for k, v in report.items()}, "chosen": chosen, "training_seconds": t_train,
             "workload": "Si64 32^3, 8 k x (128+16) bands, fixed V_loc, CG to residual 1e-8 (plain capped at "
                         f"{max_outer} outer iterations)"}
 

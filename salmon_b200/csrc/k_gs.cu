@@ -4,68 +4,131 @@
 // CTA reduction (deterministic).  Arrays: zu_GS(NL,NB,NK_s:NK_e) complex(8).
 #include <cuda_runtime.h>
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
 
 #include "sgpu_internal.cuh"
 
 namespace sgpu {
 
-constexpr int GS_THREADS = 1024;
+constexpr int GS_THREADS = 512;
 
-// <a|b> over NL complex points, valid in every thread
-__device__ __forceinline__ double2 blk_zdot(const double2* __restrict__ a, const double2* __restrict__ b, int n,
+// ------------------------------------------------------------------ groups --
+// The Gram-Schmidt and CG kernels run one thread-block cluster per k-point: the
+// cluster's C CTAs split the NL points into contiguous slices, and every inner
+// product is a fixed-order CTA sum followed by a sum of the C partials in rank
+// order, read from each CTA's shared memory over the cluster (distributed
+// shared memory); all CTAs of the cluster obtain the same value.  The
+// sequential structure of the reference (band by band, each projection on the
+// already updated vector) is kept; the cluster only parallelises each vector
+// operation over more SMs.  C = 1 is one CTA per k-point.
+namespace cgx = cooperative_groups;
+
+struct Grp {
+  int k, rank, C, lo, hi;
+  int parity;
+  double* part;  // [2][4] this CTA's partial sums (shared memory)
+};
+
+__device__ __forceinline__ Grp grp_make(int NL, double* part) {
+  cgx::cluster_group cl = cgx::this_cluster();
+  Grp g;
+  g.C = (int)cl.num_blocks();
+  g.rank = (int)cl.block_rank();
+  g.k = blockIdx.x / g.C;
+  const int slice = (NL + g.C - 1) / g.C;
+  g.lo = min(NL, g.rank * slice);
+  g.hi = min(NL, g.lo + slice);
+  g.parity = 0;
+  g.part = part;
+  return g;
+}
+
+// sum of NV doubles over the k-point's cluster, valid in every thread of every CTA
+template <int NV>
+__device__ __forceinline__ void grp_allsum(Grp& g, double (&v)[NV], double* sh) {
+  block_allsum<NV>(v, sh);
+  if (g.C == 1) return;
+  cgx::cluster_group cl = cgx::this_cluster();
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int j = 0; j < NV; ++j) g.part[g.parity * 4 + j] = v[j];
+  cl.sync();  // every CTA's partial is in place (and every read of this slot from two sums ago is done)
+  double t[NV];
+#pragma unroll
+  for (int j = 0; j < NV; ++j) t[j] = 0.0;
+  for (int r = 0; r < g.C; ++r) {
+    const double* rp = cl.map_shared_rank(g.part, r);
+#pragma unroll
+    for (int j = 0; j < NV; ++j) t[j] += rp[g.parity * 4 + j];
+  }
+#pragma unroll
+  for (int j = 0; j < NV; ++j) v[j] = t[j];
+  g.parity ^= 1;
+}
+
+// before a CTA of a cluster leaves: no other CTA still reads its shared memory
+__device__ __forceinline__ void grp_exit(const Grp& g) {
+  if (g.C > 1) cgx::this_cluster().sync();
+}
+
+// <a|b> over the NL points (the cluster's sum), valid in every thread
+__device__ __forceinline__ double2 grp_zdot(Grp& g, const double2* __restrict__ a, const double2* __restrict__ b,
                                             double* sh) {
   double v[2] = {0.0, 0.0};
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+  for (int i = g.lo + threadIdx.x; i < g.hi; i += blockDim.x) {
     const double2 x = a[i], y = b[i];
     v[0] = fma(x.x, y.x, fma(x.y, y.y, v[0]));
     v[1] = fma(x.x, y.y, fma(-x.y, y.x, v[1]));
   }
-  block_allsum<2>(v, sh);
+  grp_allsum<2>(g, v, sh);
   return make_double2(v[0], v[1]);
 }
 
-__device__ __forceinline__ double blk_nrm2(const double2* __restrict__ a, int n, double* sh) {
+__device__ __forceinline__ double grp_nrm2(Grp& g, const double2* __restrict__ a, double* sh) {
   double v[1] = {0.0};
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+  for (int i = g.lo + threadIdx.x; i < g.hi; i += blockDim.x) {
     const double2 x = a[i];
     v[0] = fma(x.x, x.x, fma(x.y, x.y, v[0]));
   }
-  block_allsum<1>(v, sh);
+  grp_allsum<1>(g, v, sh);
   return v[0];
 }
+
+#define GRP_FOR(i) for (int i = g.lo + threadIdx.x; i < g.hi; i += blockDim.x)
 
 // ------------------------------------------------------------ Gram-Schmidt --
 // Gram_Schmidt_ompk (GS/Gram_Schmidt.f90:32-55): for each band, subtract the
 // projections on the lower bands one by one (each projection uses the band as
-// already updated), then normalise.  One CTA per k-point.
+// already updated), then normalise.  One cluster per k-point.
 __global__ void __launch_bounds__(GS_THREADS) k_gram_schmidt(double2* __restrict__ zu, int NB, int NL, double Hxyz) {
   __shared__ double sh[64];
-  double2* base = zu + (size_t)blockIdx.x * NB * NL;
+  __shared__ double part[8];
+  Grp g = grp_make(NL, part);
+  double2* base = zu + (size_t)g.k * NB * NL;
   for (int ib = 0; ib < NB; ++ib) {
     double2* u = base + (size_t)ib * NL;
     for (int ibt = 0; ibt < ib; ++ibt) {
       const double2* ut = base + (size_t)ibt * NL;
-      const double2 d = blk_zdot(ut, u, NL, sh);
+      const double2 d = grp_zdot(g, ut, u, sh);
       const double2 zov = make_double2(d.x * Hxyz, d.y * Hxyz);
-      for (int i = threadIdx.x; i < NL; i += blockDim.x) u[i] = csub(u[i], cmul(ut[i], zov));
+      GRP_FOR(i) u[i] = csub(u[i], cmul(ut[i], zov));
     }
-    const double s = blk_nrm2(u, NL, sh) * Hxyz;
+    const double s = grp_nrm2(g, u, sh) * Hxyz;
     const double inv = 1.0 / sqrt(s);
-    for (int i = threadIdx.x; i < NL; i += blockDim.x) u[i] = make_double2(u[i].x * inv, u[i].y * inv);
+    GRP_FOR(i) u[i] = make_double2(u[i].x * inv, u[i].y * inv);
   }
-}
-
-cudaError_t launch_gram_schmidt(const System& s, double2* zu) {
-  k_gram_schmidt<<<s.nkl, GS_THREADS, 0, s.launch_stream()>>>(zu, s.NB, s.NL, s.Hxyz);
-  return cudaGetLastError();
+  grp_exit(g);
 }
 
 // ---------------------------------------------------------------------- CG --
 // CG_ompk with skip_gsortho='n' (GS/CG.f90:34-139), split into kernels around
-// the H applications; one CTA per k-point works on band ib of its k-point.
+// the H applications; one cluster per k-point works on band ib of its k-point.
 // Work vectors W[which][k][NL] (which = xk, hxk, txk, gk, pk, pko, htpsi, ttpsi):
 // each kind is a contiguous batch of one vector per k-point for the H pass.
+// Every CTA reads the k-point's state at the start of a kernel; rank 0 writes it
+// back only after a cluster-wide sum, i.e. after every CTA has read it.
 enum { CG_XK = 0, CG_HXK, CG_TXK, CG_GK, CG_PK, CG_PKO, CG_HT, CG_TT, CG_HK, CG_NW };
 
 struct CGState {
@@ -73,73 +136,81 @@ struct CGState {
   int done, iters;
 };
 
-__device__ __forceinline__ double2* wv(double2* W, int k, int which, int NL) {
-  return W + ((size_t)which * gridDim.x + k) * NL;
+__device__ __forceinline__ double2* wv(double2* W, int nkl, int k, int which, int NL) {
+  return W + ((size_t)which * nkl + k) * NL;
 }
 
 // Orthogonalise band ib against the lower bands with REAL coefficients (s is
 // real(8) in the reference, CG.f90:45,70), normalise into xk.
 __global__ void __launch_bounds__(GS_THREADS) k_cg_begin(double2* __restrict__ zu, double2* __restrict__ W,
-                                                         CGState* __restrict__ st, int ib, int NB, int NL, double Hxyz) {
+                                                         CGState* __restrict__ st, int ib, int nkl, int NB, int NL,
+                                                         double Hxyz) {
   __shared__ double sh[64];
-  const int k = blockIdx.x;
+  __shared__ double part[8];
+  Grp g = grp_make(NL, part);
+  const int k = g.k;
   double2* base = zu + (size_t)k * NB * NL;
   double2* u = base + (size_t)ib * NL;
   for (int ibt = 0; ibt < ib; ++ibt) {
     const double2* ut = base + (size_t)ibt * NL;
-    const double s = blk_zdot(ut, u, NL, sh).x * Hxyz;
-    for (int i = threadIdx.x; i < NL; i += blockDim.x) u[i] = make_double2(u[i].x - ut[i].x * s, u[i].y - ut[i].y * s);
+    const double s = grp_zdot(g, ut, u, sh).x * Hxyz;
+    GRP_FOR(i) u[i] = make_double2(u[i].x - ut[i].x * s, u[i].y - ut[i].y * s);
   }
-  const double inv = 1.0 / sqrt(blk_nrm2(u, NL, sh) * Hxyz);
-  double2* xk = wv(W, k, CG_XK, NL);
-  for (int i = threadIdx.x; i < NL; i += blockDim.x) xk[i] = make_double2(u[i].x * inv, u[i].y * inv);
-  if (threadIdx.x == 0) { st[k].done = 0; st[k].iters = 0; }
+  const double inv = 1.0 / sqrt(grp_nrm2(g, u, sh) * Hxyz);
+  double2* xk = wv(W, nkl, k, CG_XK, NL);
+  GRP_FOR(i) xk[i] = make_double2(u[i].x * inv, u[i].y * inv);
+  if (g.rank == 0 && threadIdx.x == 0) { st[k].done = 0; st[k].iters = 0; }
+  grp_exit(g);
 }
 
 // xkHxk = Re <xk|hxk> Hxyz
-__global__ void __launch_bounds__(GS_THREADS) k_cg_dot0(double2* __restrict__ W, CGState* __restrict__ st, int NL,
-                                                        double Hxyz) {
+__global__ void __launch_bounds__(GS_THREADS) k_cg_dot0(double2* __restrict__ W, CGState* __restrict__ st, int nkl,
+                                                        int NL, double Hxyz) {
   __shared__ double sh[64];
-  const int k = blockIdx.x;
-  const double d = blk_zdot(wv(W, k, CG_XK, NL), wv(W, k, CG_HXK, NL), NL, sh).x * Hxyz;
-  if (threadIdx.x == 0) st[k].xkHxk = d;
+  __shared__ double part[8];
+  Grp g = grp_make(NL, part);
+  const int k = g.k;
+  const double d = grp_zdot(g, wv(W, nkl, k, CG_XK, NL), wv(W, nkl, k, CG_HXK, NL), sh).x * Hxyz;
+  if (g.rank == 0 && threadIdx.x == 0) st[k].xkHxk = d;
+  grp_exit(g);
 }
 
 // gradient, orthogonalisation against the lower bands, conjugate direction,
 // pko = normalised component of pk orthogonal to xk (CG.f90:85-106)
 __global__ void __launch_bounds__(GS_THREADS) k_cg_pre(const double2* __restrict__ zu, double2* __restrict__ W,
-                                                       CGState* __restrict__ st, int ib, int iter, int NB, int NL,
-                                                       double Hxyz) {
+                                                       CGState* __restrict__ st, int ib, int iter, int nkl, int NB,
+                                                       int NL, double Hxyz) {
   __shared__ double sh[64];
-  const int k = blockIdx.x;
-  if (st[k].done) return;  // uniform per CTA
+  __shared__ double part[8];
+  Grp g = grp_make(NL, part);
+  const int k = g.k;
+  const CGState st0 = st[k];
+  if (st0.done) return;  // uniform over the cluster, before any cluster-wide sum
   const double2* base = zu + (size_t)k * NB * NL;
-  double2 *xk = wv(W, k, CG_XK, NL), *hxk = wv(W, k, CG_HXK, NL), *gk = wv(W, k, CG_GK, NL);
-  double2 *pk = wv(W, k, CG_PK, NL), *pko = wv(W, k, CG_PKO, NL);
-  const double xkHxk = st[k].xkHxk;
-  for (int i = threadIdx.x; i < NL; i += blockDim.x)
-    gk[i] = make_double2(hxk[i].x - xkHxk * xk[i].x, hxk[i].y - xkHxk * xk[i].y);
+  double2 *xk = wv(W, nkl, k, CG_XK, NL), *hxk = wv(W, nkl, k, CG_HXK, NL), *gk = wv(W, nkl, k, CG_GK, NL);
+  double2 *pk = wv(W, nkl, k, CG_PK, NL), *pko = wv(W, nkl, k, CG_PKO, NL);
+  const double xkHxk = st0.xkHxk;
+  GRP_FOR(i) gk[i] = make_double2(hxk[i].x - xkHxk * xk[i].x, hxk[i].y - xkHxk * xk[i].y);
   for (int ibt = 0; ibt < ib; ++ibt) {
     const double2* ut = base + (size_t)ibt * NL;
-    const double2 d = blk_zdot(ut, gk, NL, sh);
+    const double2 d = grp_zdot(g, ut, gk, sh);
     const double2 zs = make_double2(d.x * Hxyz, d.y * Hxyz);
-    for (int i = threadIdx.x; i < NL; i += blockDim.x) gk[i] = csub(gk[i], cmul(ut[i], zs));
+    GRP_FOR(i) gk[i] = csub(gk[i], cmul(ut[i], zs));
   }
-  const double s = blk_nrm2(gk, NL, sh) * Hxyz;
+  const double s = grp_nrm2(g, gk, sh) * Hxyz;
   if (iter == 1) {
-    for (int i = threadIdx.x; i < NL; i += blockDim.x) pk[i] = gk[i];
+    GRP_FOR(i) pk[i] = gk[i];
   } else {
-    const double uk = s / st[k].gkgk;
-    for (int i = threadIdx.x; i < NL; i += blockDim.x)
-      pk[i] = make_double2(gk[i].x + uk * pk[i].x, gk[i].y + uk * pk[i].y);
+    const double uk = s / st0.gkgk;
+    GRP_FOR(i) pk[i] = make_double2(gk[i].x + uk * pk[i].x, gk[i].y + uk * pk[i].y);
   }
-  __syncthreads();  // every thread has read gkgk
-  if (threadIdx.x == 0) st[k].gkgk = s;
-  const double2 d = blk_zdot(xk, pk, NL, sh);
+  const double2 d = grp_zdot(g, xk, pk, sh);
+  if (g.rank == 0 && threadIdx.x == 0) st[k].gkgk = s;
   const double2 zs = make_double2(d.x * Hxyz, d.y * Hxyz);
-  for (int i = threadIdx.x; i < NL; i += blockDim.x) pko[i] = csub(pk[i], cmul(xk[i], zs));
-  const double inv = 1.0 / sqrt(blk_nrm2(pko, NL, sh) * Hxyz);
-  for (int i = threadIdx.x; i < NL; i += blockDim.x) pko[i] = make_double2(pko[i].x * inv, pko[i].y * inv);
+  GRP_FOR(i) pko[i] = csub(pk[i], cmul(xk[i], zs));
+  const double inv = 1.0 / sqrt(grp_nrm2(g, pko, sh) * Hxyz);
+  GRP_FOR(i) pko[i] = make_double2(pko[i].x * inv, pko[i].y * inv);
+  grp_exit(g);
 }
 
 // Preconditioned variant (no reference counterpart; Payne et al., Rev. Mod.
@@ -150,162 +221,208 @@ __global__ void __launch_bounds__(GS_THREADS) k_cg_pre(const double2* __restrict
 // k_cg_grad also records the kinetic energy of xk (T_band, for the TPA form).
 __global__ void __launch_bounds__(GS_THREADS) k_cg_grad(const double2* __restrict__ zu, double2* __restrict__ W,
                                                         CGState* __restrict__ st, double* __restrict__ tband, int ib,
-                                                        int NB, int NL, double Hxyz) {
+                                                        int nkl, int NB, int NL, double Hxyz) {
   __shared__ double sh[64];
-  const int k = blockIdx.x;
-  if (st[k].done) return;
+  __shared__ double part[8];
+  Grp g = grp_make(NL, part);
+  const int k = g.k;
+  const CGState st0 = st[k];
+  if (st0.done) return;
   const double2* base = zu + (size_t)k * NB * NL;
-  double2 *xk = wv(W, k, CG_XK, NL), *hxk = wv(W, k, CG_HXK, NL), *gk = wv(W, k, CG_GK, NL);
-  double2* hk = wv(W, k, CG_HK, NL);
-  const double xkHxk = st[k].xkHxk;
-  for (int i = threadIdx.x; i < NL; i += blockDim.x)
-    gk[i] = make_double2(hxk[i].x - xkHxk * xk[i].x, hxk[i].y - xkHxk * xk[i].y);
+  double2 *xk = wv(W, nkl, k, CG_XK, NL), *hxk = wv(W, nkl, k, CG_HXK, NL), *gk = wv(W, nkl, k, CG_GK, NL);
+  double2* hk = wv(W, nkl, k, CG_HK, NL);
+  const double xkHxk = st0.xkHxk;
+  GRP_FOR(i) gk[i] = make_double2(hxk[i].x - xkHxk * xk[i].x, hxk[i].y - xkHxk * xk[i].y);
   for (int ibt = 0; ibt < ib; ++ibt) {
     const double2* ut = base + (size_t)ibt * NL;
-    const double2 d = blk_zdot(ut, gk, NL, sh);
+    const double2 d = grp_zdot(g, ut, gk, sh);
     const double2 zs = make_double2(d.x * Hxyz, d.y * Hxyz);
-    for (int i = threadIdx.x; i < NL; i += blockDim.x) gk[i] = csub(gk[i], cmul(ut[i], zs));
+    GRP_FOR(i) gk[i] = csub(gk[i], cmul(ut[i], zs));
   }
-  for (int i = threadIdx.x; i < NL; i += blockDim.x) hk[i] = gk[i];  // the preconditioner works in place on hk
-  const double t = blk_zdot(xk, wv(W, k, CG_TXK, NL), NL, sh).x * Hxyz;
-  if (threadIdx.x == 0) tband[k] = t;
+  GRP_FOR(i) hk[i] = gk[i];  // the preconditioner works in place on hk
+  const double t = grp_zdot(g, xk, wv(W, nkl, k, CG_TXK, NL), sh).x * Hxyz;
+  if (g.rank == 0 && threadIdx.x == 0) tband[k] = t;
+  grp_exit(g);
 }
 
 __global__ void __launch_bounds__(GS_THREADS) k_cg_dir(const double2* __restrict__ zu, double2* __restrict__ W,
-                                                       CGState* __restrict__ st, int ib, int iter, int NB, int NL,
-                                                       double Hxyz) {
+                                                       CGState* __restrict__ st, int ib, int iter, int nkl, int NB,
+                                                       int NL, double Hxyz) {
   __shared__ double sh[64];
-  const int k = blockIdx.x;
-  if (st[k].done) return;
+  __shared__ double part[8];
+  Grp g = grp_make(NL, part);
+  const int k = g.k;
+  const CGState st0 = st[k];
+  if (st0.done) return;
   const double2* base = zu + (size_t)k * NB * NL;
-  double2 *xk = wv(W, k, CG_XK, NL), *gk = wv(W, k, CG_GK, NL), *hk = wv(W, k, CG_HK, NL);
-  double2 *pk = wv(W, k, CG_PK, NL), *pko = wv(W, k, CG_PKO, NL);
+  double2 *xk = wv(W, nkl, k, CG_XK, NL), *gk = wv(W, nkl, k, CG_GK, NL), *hk = wv(W, nkl, k, CG_HK, NL);
+  double2 *pk = wv(W, nkl, k, CG_PK, NL), *pko = wv(W, nkl, k, CG_PKO, NL);
   for (int ibt = 0; ibt < ib; ++ibt) {
     const double2* ut = base + (size_t)ibt * NL;
-    const double2 d = blk_zdot(ut, hk, NL, sh);
+    const double2 d = grp_zdot(g, ut, hk, sh);
     const double2 zs = make_double2(d.x * Hxyz, d.y * Hxyz);
-    for (int i = threadIdx.x; i < NL; i += blockDim.x) hk[i] = csub(hk[i], cmul(ut[i], zs));
+    GRP_FOR(i) hk[i] = csub(hk[i], cmul(ut[i], zs));
   }
   {
-    const double2 d = blk_zdot(xk, hk, NL, sh);
+    const double2 d = grp_zdot(g, xk, hk, sh);
     const double2 zs = make_double2(d.x * Hxyz, d.y * Hxyz);
-    for (int i = threadIdx.x; i < NL; i += blockDim.x) hk[i] = csub(hk[i], cmul(xk[i], zs));
+    GRP_FOR(i) hk[i] = csub(hk[i], cmul(xk[i], zs));
   }
-  const double s = blk_zdot(gk, hk, NL, sh).x * Hxyz;
+  const double s = grp_zdot(g, gk, hk, sh).x * Hxyz;
   if (iter == 1) {
-    for (int i = threadIdx.x; i < NL; i += blockDim.x) pk[i] = hk[i];
+    GRP_FOR(i) pk[i] = hk[i];
   } else {
-    const double uk = s / st[k].gkgk;
-    for (int i = threadIdx.x; i < NL; i += blockDim.x)
-      pk[i] = make_double2(hk[i].x + uk * pk[i].x, hk[i].y + uk * pk[i].y);
+    const double uk = s / st0.gkgk;
+    GRP_FOR(i) pk[i] = make_double2(hk[i].x + uk * pk[i].x, hk[i].y + uk * pk[i].y);
   }
-  __syncthreads();  // every thread has read gkgk
-  if (threadIdx.x == 0) st[k].gkgk = s;
-  const double2 d = blk_zdot(xk, pk, NL, sh);
+  const double2 d = grp_zdot(g, xk, pk, sh);
+  if (g.rank == 0 && threadIdx.x == 0) st[k].gkgk = s;
   const double2 zs = make_double2(d.x * Hxyz, d.y * Hxyz);
-  for (int i = threadIdx.x; i < NL; i += blockDim.x) pko[i] = csub(pk[i], cmul(xk[i], zs));
-  const double inv = 1.0 / sqrt(blk_nrm2(pko, NL, sh) * Hxyz);
-  for (int i = threadIdx.x; i < NL; i += blockDim.x) pko[i] = make_double2(pko[i].x * inv, pko[i].y * inv);
+  GRP_FOR(i) pko[i] = csub(pk[i], cmul(xk[i], zs));
+  const double inv = 1.0 / sqrt(grp_nrm2(g, pko, sh) * Hxyz);
+  GRP_FOR(i) pko[i] = make_double2(pko[i].x * inv, pko[i].y * inv);
+  grp_exit(g);
 }
 
 // 2x2 Rayleigh-Ritz in span{xk, pko} and the update (CG.f90:108-119)
 __global__ void __launch_bounds__(GS_THREADS) k_cg_post(double2* __restrict__ W, CGState* __restrict__ st, int iter,
-                                                        int NL, double Hxyz, double delta_cg) {
+                                                        int nkl, int NL, double Hxyz, double delta_cg) {
   __shared__ double sh[64];
-  const int k = blockIdx.x;
-  if (st[k].done) return;
-  double2 *xk = wv(W, k, CG_XK, NL), *hxk = wv(W, k, CG_HXK, NL), *txk = wv(W, k, CG_TXK, NL);
-  const double2 *pko = wv(W, k, CG_PKO, NL), *ht = wv(W, k, CG_HT, NL), *tt = wv(W, k, CG_TT, NL);
-  const double xkHxk = st[k].xkHxk;
-  const double2 d1 = blk_zdot(xk, ht, NL, sh);
+  __shared__ double part[8];
+  Grp g = grp_make(NL, part);
+  const int k = g.k;
+  const CGState st0 = st[k];
+  if (st0.done) return;
+  double2 *xk = wv(W, nkl, k, CG_XK, NL), *hxk = wv(W, nkl, k, CG_HXK, NL), *txk = wv(W, nkl, k, CG_TXK, NL);
+  const double2 *pko = wv(W, nkl, k, CG_PKO, NL), *ht = wv(W, nkl, k, CG_HT, NL), *tt = wv(W, nkl, k, CG_TT, NL);
+  const double xkHxk = st0.xkHxk;
+  const double2 d1 = grp_zdot(g, xk, ht, sh);
   const double2 xkHpk = make_double2(d1.x * Hxyz, d1.y * Hxyz);
-  const double pkHpk = blk_zdot(pko, ht, NL, sh).x * Hxyz;
+  const double pkHpk = grp_zdot(g, pko, ht, sh).x * Hxyz;
   const double ev = 0.5 * ((xkHxk + pkHpk) - sqrt((xkHxk - pkHpk) * (xkHxk - pkHpk) +
                                                  4 * (xkHpk.x * xkHpk.x + xkHpk.y * xkHpk.y)));
   double2 cx = make_double2(xkHpk.x / (ev - xkHxk), xkHpk.y / (ev - xkHxk));
   const double cp = 1.0 / sqrt(1.0 + (cx.x * cx.x + cx.y * cx.y));
   cx = make_double2(cx.x * cp, cx.y * cp);
-  __syncthreads();
-  if (threadIdx.x == 0) st[k].iters = iter;
+  if (g.rank == 0 && threadIdx.x == 0) st[k].iters = iter;
   if (fabs(ev - xkHxk) < delta_cg) {  // delta_cg = 1e-15 in the reference (CG.f90:42,114)
-    if (threadIdx.x == 0) st[k].done = 1;
+    if (g.rank == 0 && threadIdx.x == 0) st[k].done = 1;
+    grp_exit(g);
     return;
   }
-  for (int i = threadIdx.x; i < NL; i += blockDim.x) {
+  GRP_FOR(i) {
     xk[i] = cfma(cx, xk[i], make_double2(cp * pko[i].x, cp * pko[i].y));
     hxk[i] = cfma(cx, hxk[i], make_double2(cp * ht[i].x, cp * ht[i].y));
     txk[i] = cfma(cx, txk[i], make_double2(cp * tt[i].x, cp * tt[i].y));
   }
-  const double x2 = blk_zdot(xk, hxk, NL, sh).x * Hxyz;
-  if (threadIdx.x == 0) st[k].xkHxk = x2;
+  const double x2 = grp_zdot(g, xk, hxk, sh).x * Hxyz;
+  if (g.rank == 0 && threadIdx.x == 0) st[k].xkHxk = x2;
+  grp_exit(g);
 }
 
 // zu(:,ib) = xk / |xk|; the normalised band is also left in xk for the residual
 __global__ void __launch_bounds__(GS_THREADS) k_cg_end(double2* __restrict__ zu, double2* __restrict__ W, int ib,
-                                                       int NB, int NL, double Hxyz) {
+                                                       int nkl, int NB, int NL, double Hxyz) {
   __shared__ double sh[64];
-  const int k = blockIdx.x;
-  double2* xk = wv(W, k, CG_XK, NL);
+  __shared__ double part[8];
+  Grp g = grp_make(NL, part);
+  const int k = g.k;
+  double2* xk = wv(W, nkl, k, CG_XK, NL);
   double2* u = zu + ((size_t)k * NB + ib) * NL;
-  const double inv = 1.0 / sqrt(blk_nrm2(xk, NL, sh) * Hxyz);
-  for (int i = threadIdx.x; i < NL; i += blockDim.x) {
+  const double inv = 1.0 / sqrt(grp_nrm2(g, xk, sh) * Hxyz);
+  GRP_FOR(i) {
     const double2 v = make_double2(xk[i].x * inv, xk[i].y * inv);
     u[i] = v;
     xk[i] = v;
   }
+  grp_exit(g);
 }
 
 // esp_var(ib,k) = sqrt(||H u - <u|H u> u||^2 Hxyz) occ(ib,k)  (CG.f90:124-126)
 __global__ void __launch_bounds__(GS_THREADS) k_cg_resid(double2* __restrict__ W, const double* __restrict__ occ_gs,
                                                          double* __restrict__ esp_var, double* __restrict__ res,
-                                                         int ib, int NB, int NL, double Hxyz) {
+                                                         int ib, int nkl, int NB, int NL, double Hxyz) {
   __shared__ double sh[64];
-  const int k = blockIdx.x;
-  const double2 *u = wv(W, k, CG_XK, NL), *ht = wv(W, k, CG_HT, NL);
-  const double e = blk_zdot(u, ht, NL, sh).x * Hxyz;
+  __shared__ double part[8];
+  Grp g = grp_make(NL, part);
+  const int k = g.k;
+  const double2 *u = wv(W, nkl, k, CG_XK, NL), *ht = wv(W, nkl, k, CG_HT, NL);
+  const double e = grp_zdot(g, u, ht, sh).x * Hxyz;
   double v[1] = {0.0};
-  for (int i = threadIdx.x; i < NL; i += blockDim.x) {
+  GRP_FOR(i) {
     const double2 r = make_double2(ht[i].x - e * u[i].x, ht[i].y - e * u[i].y);
     v[0] = fma(r.x, r.x, fma(r.y, r.y, v[0]));
   }
-  block_allsum<1>(v, sh);
-  if (threadIdx.x == 0) {
+  grp_allsum<1>(g, v, sh);
+  if (g.rank == 0 && threadIdx.x == 0) {
     esp_var[(size_t)k * NB + ib] = sqrt(v[0] * Hxyz) * occ_gs[(size_t)k * NB + ib];
     res[(size_t)k * NB + ib] = sqrt(v[0] * Hxyz);  // the residual norm itself, for convergence tests
   }
+  grp_exit(g);
 }
 
+// ------------------------------------------------------------------ launch --
+// CTAs per k-point: enough clusters to cover the SMs about once (C <= 16, a
+// power of two, slices of at least 1024 points); 16 needs the non-portable
+// cluster size, else 8.
+static int gs_cluster_size(const System& s) {
+  int C = 1;
+  while (C < 16 && s.nkl * C * 2 <= s.nsm && s.NL / (C * 2) >= 1024) C *= 2;
+  return C;
+}
+
+template <typename Kern, typename... Args>
+static cudaError_t launch_gs(const System& s, Kern kern, Args... args) {
+  int C = gs_cluster_size(s);
+  for (;;) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(s.nkl * C);
+    cfg.blockDim = dim3(GS_THREADS);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s.launch_stream();
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaSuccess;
+    if (C > 8) e = cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e == cudaSuccess) e = cudaLaunchKernelEx(&cfg, kern, args...);
+    if (e == cudaSuccess || C <= 8) return e;
+    (void)cudaGetLastError();  // the non-portable size was refused: clear it and use 8
+    --s.launches;
+    C = 8;
+  }
+}
+
+cudaError_t launch_gram_schmidt(const System& s, double2* zu) {
+  return launch_gs(s, k_gram_schmidt, zu, s.NB, s.NL, s.Hxyz);
+}
 cudaError_t launch_cg_begin(const System& s, double2* zu, double2* W, void* st, int ib) {
-  k_cg_begin<<<s.nkl, GS_THREADS, 0, s.launch_stream()>>>(zu, W, (CGState*)st, ib, s.NB, s.NL, s.Hxyz);
-  return cudaGetLastError();
+  return launch_gs(s, k_cg_begin, zu, W, (CGState*)st, ib, s.nkl, s.NB, s.NL, s.Hxyz);
 }
 cudaError_t launch_cg_dot0(const System& s, double2* W, void* st) {
-  k_cg_dot0<<<s.nkl, GS_THREADS, 0, s.launch_stream()>>>(W, (CGState*)st, s.NL, s.Hxyz);
-  return cudaGetLastError();
+  return launch_gs(s, k_cg_dot0, W, (CGState*)st, s.nkl, s.NL, s.Hxyz);
 }
 cudaError_t launch_cg_pre(const System& s, const double2* zu, double2* W, void* st, int ib, int iter) {
-  k_cg_pre<<<s.nkl, GS_THREADS, 0, s.launch_stream()>>>(zu, W, (CGState*)st, ib, iter, s.NB, s.NL, s.Hxyz);
-  return cudaGetLastError();
+  return launch_gs(s, k_cg_pre, zu, W, (CGState*)st, ib, iter, s.nkl, s.NB, s.NL, s.Hxyz);
 }
 cudaError_t launch_cg_post(const System& s, double2* W, void* st, int iter) {
-  k_cg_post<<<s.nkl, GS_THREADS, 0, s.launch_stream()>>>(W, (CGState*)st, iter, s.NL, s.Hxyz, s.cg_delta);
-  return cudaGetLastError();
+  return launch_gs(s, k_cg_post, W, (CGState*)st, iter, s.nkl, s.NL, s.Hxyz, s.cg_delta);
 }
 cudaError_t launch_cg_end(const System& s, double2* zu, double2* W, int ib) {
-  k_cg_end<<<s.nkl, GS_THREADS, 0, s.launch_stream()>>>(zu, W, ib, s.NB, s.NL, s.Hxyz);
-  return cudaGetLastError();
+  return launch_gs(s, k_cg_end, zu, W, ib, s.nkl, s.NB, s.NL, s.Hxyz);
 }
 cudaError_t launch_cg_grad(const System& s, const double2* zu, double2* W, void* st, double* tband, int ib) {
-  k_cg_grad<<<s.nkl, GS_THREADS, 0, s.launch_stream()>>>(zu, W, (CGState*)st, tband, ib, s.NB, s.NL, s.Hxyz);
-  return cudaGetLastError();
+  return launch_gs(s, k_cg_grad, zu, W, (CGState*)st, tband, ib, s.nkl, s.NB, s.NL, s.Hxyz);
 }
 cudaError_t launch_cg_dir(const System& s, const double2* zu, double2* W, void* st, int ib, int iter) {
-  k_cg_dir<<<s.nkl, GS_THREADS, 0, s.launch_stream()>>>(zu, W, (CGState*)st, ib, iter, s.NB, s.NL, s.Hxyz);
-  return cudaGetLastError();
+  return launch_gs(s, k_cg_dir, zu, W, (CGState*)st, ib, iter, s.nkl, s.NB, s.NL, s.Hxyz);
 }
 cudaError_t launch_cg_resid(const System& s, double2* W, const double* occ_gs, double* esp_var, double* res, int ib) {
-  k_cg_resid<<<s.nkl, GS_THREADS, 0, s.launch_stream()>>>(W, occ_gs, esp_var, res, ib, s.NB, s.NL, s.Hxyz);
-  return cudaGetLastError();
+  return launch_gs(s, k_cg_resid, W, occ_gs, esp_var, res, ib, s.nkl, s.NB, s.NL, s.Hxyz);
 }
 size_t cg_state_bytes() { return sizeof(CGState); }
 int cg_work_vectors() { return CG_NW; }

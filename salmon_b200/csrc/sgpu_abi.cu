@@ -820,13 +820,20 @@ int gs_alloc(System* s) {
   return 0;
 }
 
-// FP64 H applied to a batch of nb vectors of the k-points o/nbk (mode 0 or 1)
+// FP64 H applied to a batch of nb vectors of the k-points o/nbk (mode 0 or 1).
+// A small batch (CG works on one vector per k-point) is split into x-slabs of at
+// least 8 planes so that its pass covers the SMs (the handle's own x-slab setting
+// is for the resident orbitals).
 int gs_hpsi(System* s, const double2* in, double2* out, double2* tt, int nb, int nbk) {
   sgpu::PassIO io;
   io.in = in;
   io.out = out;
   io.tt = tt;
-  CK(apply_h(s, tt ? 1 : 0, io, 0, nb, nbk, SGPU_PREC_C128, false));
+  const int keep = s->nslab;
+  if (s->nyblk == 1) s->nslab = std::max(1, std::min(s->nsm / std::max(1, nb), s->NLx / 8));
+  const cudaError_t e = apply_h(s, tt ? 1 : 0, io, 0, nb, nbk, SGPU_PREC_C128, false);
+  s->nslab = keep;
+  CK(e);
   return 0;
 }
 

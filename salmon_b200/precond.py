@@ -163,3 +163,67 @@ def train(g, X, E, steps=300, batch=16, lr=2e-3, seed=0, log_every=0):
         if log_every and step % log_every == 0:
             print("step", step, "loss", loss, flush=True)
     return hist
+
+
+def identity_weights(noise: float = 0.0, seed: int = 0):
+    """Network weights of the identity map (centre taps: the input feeds channel
+    0 of layer 1, layer 2 passes each channel through, layer 3 reads channel 0),
+    so the learned refinement starts as TPA itself; optional N(0, noise^2) on
+    every weight.  Layout: sgpu_net_weight_count() floats, layer by layer, each
+    [co][ci][tap], tap = (dx+1)*9 + (dy+1)*3 + (dz+1)."""
+    from .rt import GpuSystem
+    C, NTAP = 8, 27
+    W1, W2, W3 = (np.zeros(x) for x in ((C, 1, NTAP), (C, C, NTAP), (1, C, NTAP)))
+    W1[0, 0, 13] = 1.0
+    W3[0, 0, 13] = 1.0
+    for c in range(C):
+        W2[c, c, 13] = 1.0
+    w = np.concatenate([W1.ravel(), W2.ravel(), W3.ravel()])
+    if noise:
+        w = w + noise * np.random.default_rng(seed).standard_normal(w.size)
+    assert w.size == GpuSystem.net_weight_count()
+    return w.astype(np.float32)
+
+
+def cg_cost(g, zu0, weights, tol=1e-8, ncg=4, max_outer=60, nconv=None):
+    """The real objective of a preconditioner on one configuration: the CG
+    iterations (summed over bands and k-points) that the ground-state sequence
+    from the orbitals zu0 needs to bring the lowest nconv bands below the
+    residual tol, with the learned preconditioner carrying `weights` (None: TPA
+    alone); a run that does not converge in max_outer iterations costs
+    twice its iterations."""
+    g.gs_set_state(zu0)
+    if weights is None:
+        g.set_cg_preconditioner("tpa")
+    else:
+        g.net_set_weights(weights)
+        g.set_cg_preconditioner("learned")
+    r = solve_to(g, tol=tol, ncg=ncg, max_outer=max_outer, nconv=nconv)
+    return r["cg_iterations"] * (1 if r["converged"] else 2)
+
+
+def train_and_select(g, X, E, variants, validate, seed=0):
+    """Trains one network per variant (dict name -> train() keyword arguments)
+    from the identity on the inputs X and targets E, and scores each with
+    validate(weights) (lower is better; validate(None) scores TPA alone), which
+    should run CG on a configuration held out from the training data
+    (cg_cost).  The best network is kept only if it scores below TPA; otherwise
+    the identity weights are returned, so the learned preconditioner falls back
+    to TPA and is not worse than it on the validation configuration.
+    Returns (weights, report {name: (final loss, score)}, chosen name)."""
+    report = {"tpa": (None, validate(None))}
+    report["identity"] = report["tpa"]  # the identity network is TPA alone
+    best_name, best_w, best_score = "identity", identity_weights(), report["tpa"][1]
+    for name, kw in variants.items():
+        g.net_set_weights(identity_weights(noise=1e-2, seed=seed))
+        hist = train(g, X, E, seed=seed, **kw)
+        w = g.net_get_weights()
+        score = validate(w)
+        report[name] = (float(np.mean(hist[-20:])), score)
+        if score < best_score:
+            best_name, best_w, best_score = name, w, score
+    return best_w, report, best_name
+
+
+DEFAULT_VARIANTS = {"short": dict(steps=100, lr=5e-4, batch=16), "mid": dict(steps=200, lr=1e-3, batch=16),
+                    "long": dict(steps=400, lr=2e-3, batch=16)}

@@ -66,7 +66,7 @@ def test_network_forward_and_gradient_match_oracle(cuda_lib):
     nv = 3
     x = rng.standard_normal((nv, sysm.NL)) + 1j * rng.standard_normal((nv, sysm.NL))
     t = rng.standard_normal((nv, sysm.NL)) + 1j * rng.standard_normal((nv, sysm.NL))
-    w = N.identity_weights(noise=0.2, seed=2)
+    w = P.identity_weights(noise=0.2, seed=2)
     g = _gpu(sysm, kAc, vloc)
     g.net_set_weights(w)
     np.testing.assert_array_equal(g.net_get_weights(), w)
@@ -101,18 +101,33 @@ def test_tpa_cg_converges_to_plain_cg_eigenvalues_in_fewer_iterations(cuda_lib):
     assert runs["tpa"]["cg_iterations"] < 0.7 * runs["plain"]["cg_iterations"]
 
 
-def test_learned_preconditioner_trains_and_cuts_cg_iterations(cuda_lib):
+def test_learned_preconditioner_trains_and_never_loses_to_its_fallback(cuda_lib):
+    """Training on residual/correction pairs from plain CG (the library's BF16
+    kernels), then selection by the real objective: a trained network is kept
+    only if its CG needs fewer iterations than TPA alone on a held-out
+    validation configuration; otherwise the identity network (= TPA) is kept.  On another configuration the result converges to the same
+    eigenvalues, in >= 30% fewer CG iterations than plain CG, and in no more
+    than 5% more than TPA alone (the selection's guarantee up to the change of
+    configuration)."""
     base = dict(SI8)
     # training data: plain CG on one displaced configuration
     sysm, kAc, vloc, zu = P.displaced_system(base, 0.05, seed=11)
     g = _gpu(sysm, kAc, vloc, zu)
     R, E, kidx, tband = P.cg_training_pairs(g, sysm, NCONV)
-    g.net_set_weights(N.identity_weights(noise=1e-2, seed=0))
-    hist = P.train(g, P.tpa_inputs(g, R, kidx, tband), E, steps=400, batch=16, lr=2e-3)
-    w = g.net_get_weights()
-    g.close()
+    X = P.tpa_inputs(g, R, kidx, tband)
+    g.net_set_weights(P.identity_weights(noise=1e-2, seed=0))
+    hist = P.train(g, X, E, steps=400, batch=16, lr=2e-3)
     print("loss", np.mean(hist[:5]), "->", np.mean(hist[-20:]))
-    assert np.mean(hist[-20:]) < 0.7 * np.mean(hist[:5])  # the network starts as TPA and fits the corrections
+    assert np.mean(hist[-20:]) < 0.7 * np.mean(hist[:5])  # the network fits the corrections
+    # validation: CG on a third configuration, held out from training and evaluation
+    vs, vk, vv, vz = P.displaced_system(base, 0.05, seed=13)
+    gv = _gpu(vs, vk, vv, vz)
+    w, report, chosen = P.train_and_select(g, X, E, P.DEFAULT_VARIANTS,
+                                           lambda wt: P.cg_cost(gv, vz, wt, max_outer=100, nconv=NCONV))
+    print("selection", report, "->", chosen)
+    assert report[chosen][1] <= report["tpa"][1]
+    gv.close()
+    g.close()
     # evaluation: another displaced configuration, converged to 1e-8
     sysm, kAc, vloc, zu = P.displaced_system(base, 0.05, seed=12)
     runs = {}
@@ -126,7 +141,5 @@ def test_learned_preconditioner_trains_and_cuts_cg_iterations(cuda_lib):
     print({k: (v["outer"], v["cg_iterations"], v["residual"]) for k, v in runs.items()})
     assert runs["learned"]["converged"] and runs["plain"]["residual"] < 1e-5
     np.testing.assert_allclose(runs["learned"]["esp"][:, :NCONV], runs["plain"]["esp"][:, :NCONV], atol=1e-9)
-    # the gain over CG without the network: >= 30% fewer CG iterations to 1e-8
     assert runs["learned"]["cg_iterations"] < 0.7 * runs["plain"]["cg_iterations"]
-    # and no worse than its fallback, TPA alone, by more than a quarter
-    assert runs["learned"]["cg_iterations"] < 1.25 * runs["tpa"]["cg_iterations"]
+    assert runs["learned"]["cg_iterations"] <= 1.05 * runs["tpa"]["cg_iterations"]
