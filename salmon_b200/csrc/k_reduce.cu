@@ -5,6 +5,8 @@
 
 #include <algorithm>
 
+#include <type_traits>
+
 #include "sgpu_internal.cuh"
 
 namespace sgpu {
@@ -216,37 +218,52 @@ __global__ void __launch_bounds__(GY / NP * GZ) k_current_march_yh(const C2<R>* 
   const int own = (h * NYH + yl) * GZ + z;                           // in the plane
   const int hrow = ((h + 1) * NYH + (t / GZ)) % GY;                   // halo row of threads t < 4 GZ
   const int hsrc = hrow * GZ + z;
+  int zo[4];                                                          // z neighbours in the staged rows
+#pragma unroll
+  for (int n = 1; n <= 4; ++n) zo[n - 1] = yl * GZ + ((z + n) % GZ);
+  // register queue: at phase P (plane x = 5i + P) plane x+m sits in q[(P+m) % 5];
+  // the march is unrolled five times so the queue rotates by renaming (NLx >= 6)
   double2 q[5];
 #pragma unroll
-  for (int m = 0; m < 5; ++m) q[m] = to_d2(__ldg(E + (size_t)(m % NLx) * NYZ + own));
+  for (int m = 0; m < 5; ++m) q[m] = to_d2(__ldg(E + (size_t)m * NYZ + own));
   C2<R> nxt = __ldg(E + (size_t)(5 % NLx) * NYZ + own);
+  int xn = 6 < NLx ? 6 : 6 - NLx;                                     // the plane loaded next
   double v[4] = {0, 0, 0, 0};
-  for (int x = 0; x < NLx; ++x) {
+  int x = 0;
+  auto step = [&](auto phase) -> bool {
+    constexpr int P = decltype(phase)::value;
     double2* pl = buf[x & 1];
-    pl[t] = q[0];
+    const double2 e = q[P % 5];
+    pl[t] = e;
     if (t < 4 * GZ) pl[NT + t] = to_d2(__ldg(E + (size_t)x * NYZ + hsrc));
     __syncthreads();
-    const double2 e = q[0];
-    v[0] += e.x * e.x + e.y * e.y;
+    v[0] = fma(e.x, e.x, fma(e.y, e.y, v[0]));
     double2 sx = make_double2(0, 0), sy = make_double2(0, 0), sz = make_double2(0, 0);
 #pragma unroll
     for (int n = 1; n <= 4; ++n) {
-      const double2 ex = q[n];
+      const double2 ex = q[(P + n) % 5];
       const double2 ey = pl[(yl + n) * GZ + z];
-      const double2 ez = pl[yl * GZ + ((z + n) % GZ)];
-      sx.x += nb[n - 1] * ex.x; sx.y += nb[n - 1] * ex.y;
-      sy.x += nb[3 + n] * ey.x; sy.y += nb[3 + n] * ey.y;
-      sz.x += nb[7 + n] * ez.x; sz.y += nb[7 + n] * ez.y;
+      const double2 ez = pl[zo[n - 1]];
+      sx.x = fma(nb[n - 1], ex.x, sx.x); sx.y = fma(nb[n - 1], ex.y, sx.y);
+      sy.x = fma(nb[3 + n], ey.x, sy.x); sy.y = fma(nb[3 + n], ey.y, sy.y);
+      sz.x = fma(nb[7 + n], ez.x, sz.x); sz.y = fma(nb[7 + n], ez.y, sz.y);
     }
-    v[1] += e.x * sx.y - e.y * sx.x;
-    v[2] += e.x * sy.y - e.y * sy.x;
-    v[3] += e.x * sz.y - e.y * sz.x;
-    q[0] = q[1];
-    q[1] = q[2];
-    q[2] = q[3];
-    q[3] = q[4];
-    q[4] = to_d2(nxt);
-    nxt = __ldg(E + (size_t)((x + 6) % NLx) * NYZ + own);
+    // aimag(conjg(e) s) = e.x s.y - e.y s.x
+    v[1] = fma(e.x, sx.y, fma(-e.y, sx.x, v[1]));
+    v[2] = fma(e.x, sy.y, fma(-e.y, sy.x, v[2]));
+    v[3] = fma(e.x, sz.y, fma(-e.y, sz.x, v[3]));
+    q[P % 5] = to_d2(nxt);  // plane x+5 takes the slot of plane x
+    nxt = __ldg(E + (size_t)xn * NYZ + own);
+    xn = xn + 1 < NLx ? xn + 1 : 0;
+    ++x;
+    return x < NLx;
+  };
+  for (;;) {
+    if (!step(std::integral_constant<int, 0>{})) break;
+    if (!step(std::integral_constant<int, 1>{})) break;
+    if (!step(std::integral_constant<int, 2>{})) break;
+    if (!step(std::integral_constant<int, 3>{})) break;
+    if (!step(std::integral_constant<int, 4>{})) break;
   }
   block_sum<4>(v, sh);
   if (t == 0) {
@@ -257,7 +274,6 @@ __global__ void __launch_bounds__(GY / NP * GZ) k_current_march_yh(const C2<R>* 
     d[3] = v[3];
   }
 }
-
 template <typename R, int GY, int GZ, int NP>
 static cudaError_t current_march_yh(System& s, const Nab12& nab, double* out) {
   k_current_march_yh<R, GY, GZ, NP><<<NP * s.norb, GY / NP * GZ, 0, s.launch_stream()>>>((const C2<R>*)s.zu, s.NLx,
@@ -551,18 +567,14 @@ static cudaError_t current_stencil(System& s, const Nab12& nab, const double* na
 // The 12 nab coefficients of the plane form live at the end of the handle's
 // reduction scratch.
 cudaError_t launch_current_stencil(System& s, double* part, int& nx) {
-  double* nab12 = s.red + (size_t)s.norb * s.NLx * 4 + 3 * (size_t)s.norb;  // [12]
-  if ((size_t)s.norb * s.NLx * 4 + 3 * (size_t)s.norb + 12 > s.red_elems) return cudaErrorInvalidValue;
-  double h[12];
-  for (int n = 0; n < 4; ++n)
-    for (int d = 0; d < 3; ++d) h[4 * d + n] = s.nab[d][n + 1];
   Nab12 nab;
-  for (int k = 0; k < 12; ++k) nab.v[k] = h[k];
+  for (int n = 0; n < 4; ++n)
+    for (int d = 0; d < 3; ++d) nab.v[4 * d + n] = s.nab[d][n + 1];
   nx = 1;
-  const cudaError_t e = cudaMemcpyAsync(nab12, h, sizeof(h), cudaMemcpyHostToDevice, s.stream);
-  if (e != cudaSuccess) return e;
-  return s.prec == SGPU_PREC_C64 ? current_stencil<float>(s, nab, nab12, part, nx)
-                                 : current_stencil<double>(s, nab, nab12, part, nx);
+  // s.nab12 (device, set at creation) for the plane form; no scratch shared with
+  // work that may run beside this on the handle's other stream
+  return s.prec == SGPU_PREC_C64 ? current_stencil<float>(s, nab, s.nab12, part, nx)
+                                 : current_stencil<double>(s, nab, s.nab12, part, nx);
 }
 
 cudaError_t launch_current(System& s, double* jav_dev) {
@@ -572,6 +584,8 @@ cudaError_t launch_current(System& s, double* jav_dev) {
   int nx = 1;
   cudaError_t e;
   if (s.cur_valid) {  // computed by the Taylor step that produced these orbitals (flag_current)
+    e = s.aux_join();
+    if (e != cudaSuccess) return e;
     part = s.cur_part;
     nx = s.cur_nx;
   } else {

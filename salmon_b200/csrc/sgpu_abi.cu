@@ -148,6 +148,8 @@ cudaError_t sgpu::enqueue_taylor_step(System& sys, double dt, bool gather_first,
 cudaError_t sgpu::enqueue_taylor_step_on(System& sys, void* zu_buf, double dt, bool gather_first,
                                          bool with_current) {
   System* s = &sys;
+  cudaError_t ej = s->aux_join();  // the previous step's stencil sums still read zu
+  if (ej != cudaSuccess) return ej;
   s->cur_valid = false;
   const bool resident = s->taylor_kernel == 2 || (s->taylor_kernel == 0 && sgpu::resident_step_default(*s));
   if (resident) {
@@ -179,9 +181,19 @@ cudaError_t sgpu::enqueue_taylor_step_on(System& sys, void* zu_buf, double dt, b
     if (e != cudaSuccess) return e;
   }
   s->S_valid = s->nsp > 0;
-  if (with_current && zu_buf == s->zu) {  // the stencil sums of the new orbitals, right after the update
+  if (with_current && zu_buf == s->zu) {
+    // the stencil sums of the new orbitals, right after the update, on the second
+    // stream: they overlap whatever the caller queues next on `stream` (the
+    // density, the nonlocal current), which only reads the orbitals too
     int nx = 1;
-    if ((e = sgpu::launch_current_stencil(*s, s->cur_part, nx)) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(s->ev_step, s->stream)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(s->aux, s->ev_step, 0)) != cudaSuccess) return e;
+    std::swap(s->stream, s->aux);
+    e = sgpu::launch_current_stencil(*s, s->cur_part, nx);
+    std::swap(s->stream, s->aux);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaEventRecord(s->ev_cur, s->aux)) != cudaSuccess) return e;
+    s->aux_pending = true;
     s->cur_nx = nx;
     s->cur_valid = true;
   }
@@ -261,6 +273,10 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
   if (e != cudaSuccess) { delete s; return cuda_fail(e, "cudaGetDevice"); }
   e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { delete s; return cuda_fail(e, "cudaStreamCreate"); }
+  if ((e = cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&s->ev_step, cudaEventDisableTiming)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&s->ev_cur, cudaEventDisableTiming)) != cudaSuccess)
+    return bail(cuda_fail(e, "sgpu_create: second stream"));
   {
     int dev = 0;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -461,6 +477,14 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
   if ((e = dalloc(&s->red, s->red_elems)) != cudaSuccess) return bail(cuda_fail(e, "alloc red"));
   if ((e = dalloc(&s->cur_part, (size_t)s->norb * s->NLx * 4)) != cudaSuccess)
     return bail(cuda_fail(e, "alloc cur_part"));
+  {
+    double h12[12];
+    for (int n = 0; n < 4; ++n)
+      for (int dd = 0; dd < 3; ++dd) h12[4 * dd + n] = s->nab[dd][n + 1];
+    if ((e = dalloc(&s->nab12, 12)) != cudaSuccess) return bail(cuda_fail(e, "alloc nab12"));
+    if ((e = cudaMemcpy(s->nab12, h12, sizeof(h12), cudaMemcpyHostToDevice)) != cudaSuccess)
+      return bail(cuda_fail(e, "copy nab12"));
+  }
   s->red_h_elems = (size_t)s->NL + 64;
   if ((e = cudaMallocHost((void**)&s->red_h, s->red_h_elems * sizeof(double))) != cudaSuccess)
     return bail(cuda_fail(e, "alloc pinned"));
@@ -484,7 +508,7 @@ int sgpu_destroy(sgpu_handle h) {
   free_state_buffers(s);
   void* bufs[] = {s->vloc64, s->vloc32, s->occ_o, s->kAc_d, s->idx_proj, s->atom_off, s->rpos, s->items,
                   s->lma_list, s->iuV_d, s->lma_atom, s->uV_d, s->zproj64, s->zproj32, s->sp_off, s->rec, s->cont, s->qmap, s->kbq, s->kb_multi, s->lqi, s->Sbuf, s->Wbuf,
-                  s->U, s->Uw, s->red, s->stage, s->cur_part};
+                  s->U, s->Uw, s->red, s->stage, s->cur_part, s->nab12};
   for (void* p : bufs) cudaFree(p);
   void* gbufs[] = {s->gs_zu, s->gs_aux, s->gs_W, s->gs_st, s->gs_part, s->gs_A, s->gs_V, s->gs_w, s->gs_sweeps,
                    s->occ_gs, s->gs_out, s->gs_res, s->gs_tb, s->vpsl, s->rho_d, s->exc_d, s->sp_blk,
@@ -492,13 +516,18 @@ int sgpu_destroy(sgpu_handle h) {
   for (void* p : gbufs) cudaFree(p);
   if (s->gs_h) cudaFreeHost(s->gs_h);
   if (s->red_h) cudaFreeHost(s->red_h);
+  if (s->aux) cudaStreamSynchronize(s->aux);
   if (s->stream) cudaStreamDestroy(s->stream);
+  if (s->aux) cudaStreamDestroy(s->aux);
+  if (s->ev_step) cudaEventDestroy(s->ev_step);
+  if (s->ev_cur) cudaEventDestroy(s->ev_cur);
   delete h;
   return 0;
 }
 
 int sgpu_synchronize(sgpu_handle h) {
   if (!valid(h)) return fail(SGPU_ERR_ARG, "null handle");
+  CK(h->aux_join());
   CK(cudaStreamSynchronize(h->stream));
   return 0;
 }
@@ -510,6 +539,7 @@ void* sgpu_state_ptr(sgpu_handle h) { return h ? h->zu : nullptr; }
 int sgpu_set_state(sgpu_handle h, const double* zu) {
   if (!valid(h) || !zu) return fail(SGPU_ERR_ARG, "sgpu_set_state: null argument");
   System* s = h;
+  CK(s->aux_join());
   const size_t n = (size_t)s->norb * s->NL;
   if (s->prec == SGPU_PREC_C128) {
     CK(cudaMemcpyAsync(s->zu, zu, n * sizeof(double2), cudaMemcpyHostToDevice, s->stream));
@@ -529,6 +559,7 @@ int sgpu_set_state(sgpu_handle h, const double* zu) {
 
 int sgpu_set_state_dev(sgpu_handle h, const void* zu_dev) {
   if (!valid(h) || !zu_dev) return fail(SGPU_ERR_ARG, "sgpu_set_state_dev: null argument");
+  CK(h->aux_join());
   System* s = h;
   const size_t n = (size_t)s->norb * s->NL;
   if (s->prec == SGPU_PREC_C128)
@@ -565,6 +596,8 @@ int sgpu_set_precision(sgpu_handle h, int precision) {
   if (precision != SGPU_PREC_C128 && precision != SGPU_PREC_C64) return fail(SGPU_ERR_ARG, "bad precision");
   System* s = h;
   if (precision == s->prec) return 0;
+  CK(s->aux_join());
+  CK(cudaStreamSynchronize(s->stream));  // zu is freed below
   const size_t n = (size_t)s->norb * s->NL;
   void* old = s->zu;
   const int old_prec = s->prec;
@@ -1029,6 +1062,7 @@ int sgpu_gs_to_rt(sgpu_handle h) {
   if (!valid(h)) return fail(SGPU_ERR_ARG, "null handle");
   System* s = h;
   if (!s->have_gs) return fail(SGPU_ERR_STATE, "sgpu_gs_to_rt: no ground-state orbitals loaded");
+  CK(s->aux_join());
   const size_t run = (size_t)s->NBocc * s->NL;
   for (int k = 0; k < s->nkl; ++k) {
     const double2* src = s->gs_zu + (size_t)k * s->NB * s->NL;

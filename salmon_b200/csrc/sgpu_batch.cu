@@ -131,6 +131,10 @@ int sgpu_batch_step(sgpu_batch_handle b, const double* dt, int nsteps) {
   for (System* s : b->sys)
     if (!s->have_state || !s->have_vloc || !s->have_proj)
       return bfail(SGPU_ERR_STATE, "sgpu_batch_step: every system needs state, Vloc and projectors");
+  for (System* s : b->sys) {  // a flag_current step's stencil sums still read the orbitals
+    cudaError_t e = s->aux_join();
+    if (e != cudaSuccess) return bcuda(e, "sgpu_batch_step: join");
+  }
   bool stale = !b->exec || b->key_steps != nsteps;
   for (size_t i = 0; i < b->sys.size() && !stale; ++i)
     stale = b->key_dt[i] != dt[i] || b->key_gen[i] != b->sys[i]->gen;

@@ -198,8 +198,22 @@ struct System {
   // Taylor step called with flag_current (RT/hamiltonian.f90:68-70): rows
   // cur_part[o][cur_nx][4], valid while cur_valid (the orbitals are unchanged since).
   double* cur_part = nullptr;      // [norb][NLx][4]
+  double* nab12 = nullptr;         // [12] nabx(1:4), naby(1:4), nabz(1:4) (device, set at creation)
   int cur_nx = 0;
   bool cur_valid = false;
+  // The stencil sums of a flag_current step run on a second stream (they only read
+  // the orbitals), overlapping the density and the nonlocal current that follow on
+  // `stream`; ev_cur marks their end.  aux_pending: `stream` has not waited for it.
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_step = nullptr, ev_cur = nullptr;
+  bool aux_pending = false;
+  // Makes `stream` wait for the stencil sums (before anything writes the orbitals
+  // or cur_part, or reads cur_part).
+  cudaError_t aux_join() {
+    if (!aux_pending) return cudaSuccess;
+    aux_pending = false;
+    return cudaStreamWaitEvent(stream, ev_cur, 0);
+  }
   int nsm = 148;                   // SMs of the device
   mutable bool kb_smem_ok = false;  // the KB tile kernels' shared-memory limits are raised for this handle
   int um_split = 4;                // band-quad KB kernel: warps splitting the points of one tile (1, 2, 4, 8)
