@@ -66,6 +66,8 @@ def parse():
     p.add_argument("--taylor-kernel", type=int, default=0, choices=[0, 1, 2],
                    help="Taylor step of the main leg: 0 by grid, 1 stencil passes, 2 shared-memory resident")
     p.add_argument("--no-si8", action="store_true", help="skip the Si8 16^3 resident-vs-passes leg")
+    p.add_argument("--config5", type=int, default=0, metavar="STEPS",
+                   help="also run the Si216 pulsed RT workload for STEPS steps (minutes; 5000 as configured)")
     p.add_argument("--kb-kernel", type=int, default=0, choices=[0, 1, 2],
                    help="KB term kernel of the main leg: 0 by grid size, 1 band-group tile, 2 band-quad (profiling)")
     return p.parse_args()
@@ -370,6 +372,97 @@ def precond_bench(max_outer=60):
                         f"{max_outer} outer iterations)"}
 
 
+def config5_bench(nsteps=5000, nscf=60, check_steps=500, npolish=3):
+    """The large pulsed RT run: Si216 (3x3x3 diamond supercell, a = 10.26 bohr),
+    48^3 grid, 2x2x1 = 4 k-points, 432 occupied bands, the physical Si
+    pseudopotential (KY, lloc = 2, the testsuites' Si_rps.dat as parsed into
+    tests/golden/si_rps_ky.npz), PZ LDA.  Ground state: the perfect crystal's
+    supercell state is the unit cell's unfolded, so the reference's SCF loop
+    (Broyden, TPA-preconditioned CG, FP64) runs on Si8 (16^3, the same spacing) at
+    the 108 unit-cell k-points that fold onto the supercell's four, its 16
+    occupied bands per k-point are unfolded onto the 48^3 grid on the device
+    (system.unfold_to_supercell) and `npolish` supercell ground-state iterations
+    remove the grid error of the unfolding.  Then `nsteps` middle-point Taylor steps of
+    dt = 0.08 in complex(4) with FP64 reductions under a cos^2-envelope pulse
+    (hbar omega = 1.55 eV, 1e12 W/cm^2, 20 fs), the Hartree + PZ potential
+    rebuilt every step on the device, J every step; the first `check_steps` steps
+    again in complex(8) for the J(t) error."""
+    import torch
+    from salmon_b200 import drive, precond as PC, pseudo as P, system as S
+    from salmon_b200.rt import GpuSystem
+    tabs = P.prepare(P.from_npz(os.path.join(ROOT, "tests", "golden", "si_rps_ky.npz"), lloc=2))
+    ncell = (3, 3, 3)
+    big, kS, vpsl, _ = S.si_pp_system(tabs, ncell=ncell, grid=(48, 48, 48), nkgrid=(2, 2, 1), NB=432, Nocc=432,
+                                      with_orbitals=False)
+    kU, ms = S.folded_kpoints(kS, ncell, big.aL)
+    cell, _, vpsl_c, zu0 = S.si_pp_system(tabs, grid=(16, 16, 16), NB=20, Nocc=16, kpoints=kU)
+    out = {"workload": "Si216 48^3, 4 k x 432 bands, physical Si pseudopotential (KY), PZ LDA; ground state "
+                       "unfolded from the Si8 SCF at the 108 folded k-points; then "
+                       f"{nsteps} complex(4) steps of dt = 0.08 under an Acos2 pulse (1.55 eV, 1e12 W/cm^2, 20 fs), "
+                       "self-consistent Vloc every step"}
+    t0 = time.perf_counter()
+    with GpuSystem(cell, "c128") as g:
+        g.gs_set_state(zu0)
+        g.set_cg_preconditioner("tpa")
+        esp, hist = drive.gs_scf(g, cell, kU, vpsl_c, nscf=nscf, ncg=4, threshold=1e-8)
+        zgs = g.gs_get_state()
+    out["ground_state"] = {"scf_iterations": len(hist), "ddns_last": hist[-1][0], "max_esp_var": hist[-1][1],
+                           "seconds": time.perf_counter() - t0,
+                           "gap_ha": float(np.sort(esp, axis=1)[:, 16].min() - np.sort(esp, axis=1)[:, 15].max())}
+    zs_t = S.unfold_to_supercell(torch.from_numpy(np.ascontiguousarray(zgs[:, :16])).cuda(), ncell, ms,
+                                 kS.shape[1], (16, 16, 16))
+    zs = zs_t.cpu().numpy()
+    del zs_t
+    # the unfolded states are the supercell's to the grid error of the k+A treatment
+    # (tests/test_unfold.py); a few supercell ground-state iterations in the
+    # unfolded state's own potential remove it
+    t0 = time.perf_counter()
+    with GpuSystem(big, "c128") as g:
+        g.set_vpsl(vpsl)
+        g.set_vloc(vpsl)
+        g.update_projector(kS)
+        g.gs_set_state(zs)
+        g.gs_to_rt()
+        g.update_vloc()
+        g.set_cg_preconditioner("tpa")
+        res0 = None
+        for it in range(npolish):
+            _, ncg_it, res = PC.gs_iteration(g, 4)
+            res0 = res if res0 is None else res0
+        zs = g.gs_get_state()
+    out["supercell_polish"] = {"iterations": npolish, "max_residual_first": res0, "max_residual_last": res,
+                               "seconds": time.perf_counter() - t0}
+    eion = P.ewald_energy(big.Rion, big.extra["zps"], big.aL, (big.NLx, big.NLy, big.NLz))
+    dt = 0.08
+    Ac = drive.init_Ac(nsteps + 1, dt, "Acos2", epdir=(0.0, 0.0, 1.0), rlaser_int_wcm2=1e12,
+                       omega=1.55 / 27.211386245988, pulse_tw=20.0 * 41.341373335)
+    runs = {}
+    for prec, n in (("c64", nsteps), ("c128", check_steps)):
+        with GpuSystem(big, "c128") as g:
+            g.set_state(zs)
+            if prec == "c64":
+                g.set_precision("c64")
+            g.update_projector(kS)
+            g.synchronize()
+            t1 = time.perf_counter()
+            javt, energies = drive.rt_propagate(g, big, kS, vpsl, Ac, dt, n, energy_every=max(1, n // 10),
+                                                scf=True, eion=eion)
+            g.synchronize()
+            sec = time.perf_counter() - t1
+        runs[prec] = (javt, energies, sec, n)
+    del zs
+    j64, e64, s64, n64 = runs["c128"]
+    j32, e32, s32, n32 = runs["c64"]
+    norb = big.nk_local * big.NBoccmax
+    out["c64"] = {"steps": n32, "seconds": s32, "ms_per_step_wall": 1e3 * s32 / n32,
+                  "orbital_updates_per_s_wall": norb * n32 / s32,
+                  "energy_change_ha": float(e32[max(e32)] - e32[0]), "max_abs_j": float(np.abs(j32).max())}
+    out["c128"] = {"steps": n64, "seconds": s64, "ms_per_step_wall": 1e3 * s64 / n64}
+    out["j_rel_err_first_steps"] = drive.j_error(j64, j32[:n64 + 1])
+    out["energy_change_abs_diff_ha"] = float(max(abs((e32[t] - e32[0]) - (e64[t] - e64[0])) for t in e64 if t in e32))
+    return out
+
+
 def si8_bench(nsteps=50):
     """The Si8 RT shape of the plain FP64 run (16^3 grid, 4x4x4 k, 16 bands, 1024
     orbitals; synthetic Gaussian projectors and V_loc): Taylor-step time of the
@@ -583,6 +676,7 @@ def main():
     if rank == 0 and not (args.only or args.no_e2e or args.no_si8):
         si8 = si8_bench()
     pc = precond_bench() if (rank == 0 and args.precond) else None
+    c5 = config5_bench(args.config5) if (rank == 0 and args.config5) else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -590,7 +684,8 @@ def main():
         except Exception as exc:  # the CPU baseline is reported, never required
             cpu = {"unavailable": str(exc)}
     if rank == 0 and (args.only or args.no_e2e):
-        print(json.dumps({p: {k: v for k, v in r.items() if k != "e2e"} for p, r in res.items()}))
+        print(json.dumps({p: {k: v for k, v in r.items() if k != "e2e"} for p, r in res.items()} |
+                         ({"config5": c5} if c5 else {})))
     elif rank == 0:
         h = res["c64"]
         tpo = NCU_TRAFFIC_BYTES_PER_ORBITAL.get(("taylor_stage", "c64", args.grid))
@@ -620,6 +715,7 @@ def main():
             "large": large,
             "si8_resident_vs_passes": si8,
             "precond": pc,
+            "config5": c5,
             "clocks": clocks,
         }
         print(json.dumps(out))

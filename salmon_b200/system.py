@@ -469,7 +469,7 @@ def small_system(NLx=8, NLy=8, NLz=10, nk=3, nb=4, a=(6.0, 6.5, 7.0), nat=2, see
 
 
 def si_pp_system(tabs, ncell=(1, 1, 1), grid=(8, 8, 8), nkgrid=(4, 4, 4), NB: int = 32, Nocc: int = 16,
-                 a: float = 10.26, seed: int = SEED, with_orbitals: bool = True):
+                 a: float = 10.26, seed: int = SEED, with_orbitals: bool = True, kpoints=None):
     """Diamond-Si supercell with the physical pseudopotential ``tabs``
     (``pseudo.prepare`` of a KY file): sphere points within the element's Rps
     (calc_jxyz), uV = spline(udV_l) x Ylm on them (calc_uv), Vpsl from the
@@ -478,13 +478,13 @@ def si_pp_system(tabs, ncell=(1, 1, 1), grid=(8, 8, 8), nkgrid=(4, 4, 4), NB: in
     (001_bulk_gs, 002_bulk_rt) is the default: 8 atoms, 8^3 grid, 4^3 k, 32 bands.
     Returns (system, kAc0 (3,NK), Vpsl (NL,), zu_GS (nk,NB,NL) or None); zu_GS
     is seeded random and orthonormal (the reference's init_wf draws random
-    orbitals too)."""
+    orbitals too).  kpoints (3, NK), if given, replaces the uniform k grid."""
     from . import pseudo as P
     nc = np.asarray(ncell)
     aL = a * nc.astype(np.float64)
     NLx, NLy, NLz = grid
     bl = 2 * np.pi / aL
-    kAc0 = uniform_k_grid(*nkgrid, bl)
+    kAc0 = uniform_k_grid(*nkgrid, bl) if kpoints is None else np.ascontiguousarray(kpoints, dtype=np.float64)
     NK = kAc0.shape[1]
     occ = np.zeros((NK, NB))
     occ[:, :Nocc] = 2.0 / NK
@@ -504,3 +504,41 @@ def si_pp_system(tabs, ncell=(1, 1, 1), grid=(8, 8, 8), nkgrid=(4, 4, 4), NB: in
         zu = rng.standard_normal((NK, NB, NL)) + 1j * rng.standard_normal((NK, NB, NL))
         zu = orthonormalise(zu, sysm.Hxyz)
     return sysm, np.ascontiguousarray(kAc0), vpsl, zu
+
+
+def folded_kpoints(ks_super, ncell, aL_super):
+    """The unit-cell k-points that fold onto the supercell k-points ks_super
+    (3, NKs) of a supercell of ncell unit cells: k_u = k_s + m b_s for every
+    m in [0, ncell), b_s = 2 pi / aL_super per axis.  Returns (3, NKs * prod(ncell))
+    ordered supercell k-point by supercell k-point, m in C order."""
+    nc = np.asarray(ncell)
+    bs = 2 * np.pi / np.asarray(aL_super, dtype=np.float64)
+    ms = np.array([[i, j, k] for i in range(nc[0]) for j in range(nc[1]) for k in range(nc[2])], dtype=np.float64)
+    out = [ks_super[:, s] + m * bs for s in range(ks_super.shape[1]) for m in ms]
+    return np.ascontiguousarray(np.array(out).T), ms.astype(np.int64)
+
+
+def unfold_to_supercell(zu_cell, ncell, ms, nks, grid_cell):
+    """Bloch-periodic parts on the supercell grid from those of the unit cell
+    (torch CUDA tensors): for supercell k-point s and unit-cell k-point
+    k_u = k_s + m b_s, u_s(R) = exp(i m b_s . R h) u_{k_u}(R mod cell) / sqrt(prod
+    ncell), an eigenstate of the supercell Hamiltonian at k_s with the same
+    eigenvalue (a perfect crystal).  zu_cell: (nks * nfold, nb, NLc) complex128;
+    returns (nks, nfold * nb, NLs) with the unit-cell k-points of one supercell
+    k-point band-block after band-block."""
+    import torch
+    nc = [int(x) for x in ncell]
+    gx, gy, gz = grid_cell
+    Sx, Sy, Sz = gx * nc[0], gy * nc[1], gz * nc[2]
+    nfold = int(np.prod(nc))
+    nb = zu_cell.shape[1]
+    out = torch.empty((nks, nfold * nb, Sx * Sy * Sz), dtype=torch.complex128, device=zu_cell.device)
+    ax = [torch.arange(n, device=zu_cell.device, dtype=torch.float64) for n in (Sx, Sy, Sz)]
+    for s in range(nks):
+        for j in range(nfold):
+            m = ms[j]
+            u = zu_cell[s * nfold + j].reshape(nb, gx, gy, gz).repeat(1, nc[0], nc[1], nc[2])
+            ph = [torch.exp(1j * 2 * np.pi * float(m[d]) * ax[d] / (nc[d] * (gx, gy, gz)[d])) for d in range(3)]
+            phase = ph[0][:, None, None] * ph[1][None, :, None] * ph[2][None, None, :]
+            out[s, j * nb:(j + 1) * nb] = (u * phase[None] / np.sqrt(nfold)).reshape(nb, -1)
+    return out
