@@ -337,8 +337,8 @@ enum {
   SGPU_PARAM_TAYLOR_KERNEL = 8, /* Taylor step: 1 four stencil passes over all orbitals (any grid), 2
                                  the orbitals of a band group resident in one CTA's shared memory for
                                  the whole step (16x16, 16x32 and 20x20 planes where they fit), 0 the
-                                 resident form where it is the faster one (complex(4), 16x16 planes),
-                                 else the passes                                                     */
+                                 resident form where it is the faster one (16x16 planes), else the
+                                 passes                                                              */
   SGPU_PARAM_NSP = 9          /* sphere points of the handle (read only): the union of the
                                  projectors' points, a key of the launch-shape table              */
 };

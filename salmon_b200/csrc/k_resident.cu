@@ -64,19 +64,20 @@ struct ResArgs {
 __host__ __device__ constexpr size_t res_align16(size_t b) { return (b + 15) & ~(size_t)15; }
 
 // NBC bands of one k-point per CTA; V_loc staged in shared memory where it fits.
-template <typename R, int GY, int GZ, int NBC_> struct ResGeom {
+template <typename R, int GY, int GZ, int NBC_, int RZ_ = 2> struct ResGeom {
   static constexpr bool c64 = std::is_same<R, float>::value;
   static constexpr int NBC = NBC_;
+  static constexpr int RZ = RZ_;                        // z points per thread
   static constexpr bool VS = c64 && GY * GZ <= 256;
-  static constexpr int NTO = ((GY * GZ / 2 + 31) / 32) * 32;  // threads per band
+  static constexpr int NTO = ((GY * GZ / RZ + 31) / 32) * 32;  // threads per band
   static constexpr int NT = NBC * NTO;
 };
 
 // shared memory: NBC orbitals, their wrap planes, W at the sphere points and U;
 // the sphere-index table, V_loc (when staged), sp_off and the reduction scratch
-template <typename R, int GY, int GZ, int NBC>
+template <typename R, int GY, int GZ, int NBC, int RZ = 2>
 __host__ __device__ inline size_t res_smem_bytes(int NLx, int nsp, int Nlma) {
-  using G = ResGeom<R, GY, GZ, NBC>;
+  using G = ResGeom<R, GY, GZ, NBC, RZ>;
   const size_t e = sizeof(C2<R>), NL = (size_t)NLx * GY * GZ;
   return G::NBC * (res_align16(e * NL) + res_align16(e * 4 * GY * GZ) + res_align16(e * (size_t)nsp) +
                    res_align16(sizeof(double2) * (size_t)Nlma)) +
@@ -93,13 +94,13 @@ __device__ __forceinline__ double warp_sum(double v) {
 // One CTA advances NBC consecutive bands of one k-point together (lockstep
 // marches, one barrier per plane for all of them), so the projector tables each
 // stage reads are shared by NBC orbitals through L1.
-template <typename R, int GY, int GZ, int NBC_>
-__global__ void __launch_bounds__(ResGeom<R, GY, GZ, NBC_>::NT, 1) k_taylor_resident(const ResArgs<R> a) {
+template <typename R, int GY, int GZ, int NBC_, int RZ_>
+__global__ void __launch_bounds__(ResGeom<R, GY, GZ, NBC_, RZ_>::NT, 1) k_taylor_resident(const ResArgs<R> a) {
   using T = C2<R>;
-  using G = ResGeom<R, GY, GZ, NBC_>;
-  constexpr int RZ = 2, NBC = G::NBC, NTO = G::NTO, NT = G::NT;
+  using G = ResGeom<R, GY, GZ, NBC_, RZ_>;
+  constexpr int RZ = G::RZ, NBC = G::NBC, NTO = G::NTO, NT = G::NT;
   constexpr int NLy = GY, NLz = GZ, NYZ = GY * GZ, NZG = GZ / RZ;
-  static_assert(GZ % 2 == 0, "two z points per thread");
+  static_assert(GZ % RZ == 0 && (RZ == 1 || RZ == 2), "one or two z points per thread");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int NLx = a.NLx, NL = a.NL;
   unsigned char* sp = smem_raw;
@@ -272,9 +273,13 @@ __global__ void __launch_bounds__(ResGeom<R, GY, GZ, NBC_>::NT, 1) k_taylor_resi
             const int xn = x + 4;
             lds_run<R, RZ>(q[(PH + 8) % 9], xn < NLx ? P + (size_t)xn * NYZ + own : wrap + (size_t)(xn - NLx) * NYZ + own);
           }
-          const int lqv = *reinterpret_cast<const int*>(lqs + (size_t)x * NYZ + own);
-          lq[0] = (int)(short)(lqv & 0xffff);
-          lq[1] = lqv >> 16;
+          if constexpr (RZ == 2) {
+            const int lqv = *reinterpret_cast<const int*>(lqs + (size_t)x * NYZ + own);
+            lq[0] = (int)(short)(lqv & 0xffff);
+            lq[1] = lqv >> 16;
+          } else {
+            lq[0] = lqs[(size_t)x * NYZ + own];
+          }
           R vl[RZ];
           if constexpr (G::VS) {
 #pragma unroll
@@ -449,14 +454,14 @@ __global__ void __launch_bounds__(ResGeom<R, GY, GZ, NBC_>::NT, 1) k_taylor_resi
 }
 
 // ------------------------------------------------------------------ launch --
-template <typename R, int GY, int GZ, int NBC>
-static size_t res_smem(const System& s) { return res_smem_bytes<R, GY, GZ, NBC>(s.NLx, s.nsp, s.Nlma); }
+template <typename R, int GY, int GZ, int NBC, int RZ = 2>
+static size_t res_smem(const System& s) { return res_smem_bytes<R, GY, GZ, NBC, RZ>(s.NLx, s.nsp, s.Nlma); }
 
-template <typename R, int GY, int GZ, int NBC>
+template <typename R, int GY, int GZ, int NBC, int RZ>
 static cudaError_t launch_res_t(const System& s, void* zu, double dt, double* cur, void* S) {
-  using G = ResGeom<R, GY, GZ, NBC>;
-  const size_t smem = res_smem<R, GY, GZ, NBC>(s);
-  auto kern = k_taylor_resident<R, GY, GZ, NBC>;
+  using G = ResGeom<R, GY, GZ, NBC, RZ>;
+  const size_t smem = res_smem<R, GY, GZ, NBC, RZ>(s);
+  auto kern = k_taylor_resident<R, GY, GZ, NBC, RZ>;
   {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     cudaError_t e = cudaStreamIsCapturing(s.stream, &cs);
@@ -508,9 +513,11 @@ static cudaError_t launch_res_t(const System& s, void* zu, double dt, double* cu
 }
 
 // The forms built for each plane shape, widest band group first:
-//   complex(4): 16x16 planes 4 or 2 bands per CTA, 16x32 and 20x20 2 or 1;
-//   complex(8): 16x16 2 or 1, 16x32 and 20x20 1.
-// f(tag, GY, GZ, NBC) is called for the first form whose shared memory fits
+//   complex(4), two z points per thread: 16x16 planes 4 or 2 bands per CTA, 16x32
+//   and 20x20 2 or 1;
+//   complex(8), one z point per thread (twice the warps of the two-point form at
+//   its register count): 16x16 planes 2 or 1 bands, 16x32 and 20x20 1.
+// f(tag, GY, GZ, NBC, RZ) is called for the first form whose shared memory fits
 // (returns false if none does).
 template <typename F>
 static bool res_dispatch(const System& s, F&& f) {
@@ -522,45 +529,45 @@ static bool res_dispatch(const System& s, F&& f) {
   using I32 = std::integral_constant<int, 32>;
   if (s.NLx < 9 || s.nsp < 1 || s.nitems < 1) return false;
   constexpr size_t cap = 227 * 1024;
-  auto fits = [&](auto tag, auto gy, auto gz, auto nbc) {
+  auto tryf = [&](auto tag, auto gy, auto gz, auto nbc, auto rz) {
     using R = decltype(tag);
-    return res_smem<R, decltype(gy)::value, decltype(gz)::value, decltype(nbc)::value>(s) <= cap;
-  };
-  auto tryf = [&](auto tag, auto gy, auto gz, auto nbc) {
-    if (!fits(tag, gy, gz, nbc)) return false;
-    f(tag, gy, gz, nbc);
+    if (res_smem<R, decltype(gy)::value, decltype(gz)::value, decltype(nbc)::value, decltype(rz)::value>(s) > cap)
+      return false;
+    f(tag, gy, gz, nbc, rz);
     return true;
   };
   if (s.prec == SGPU_PREC_C64) {
-    if (s.NLy == 16 && s.NLz == 16) return tryf(0.0f, I16{}, I16{}, I4{}) || tryf(0.0f, I16{}, I16{}, I2{});
-    if (s.NLy == 16 && s.NLz == 32) return tryf(0.0f, I16{}, I32{}, I2{}) || tryf(0.0f, I16{}, I32{}, I1{});
-    if (s.NLy == 20 && s.NLz == 20) return tryf(0.0f, I20{}, I20{}, I2{}) || tryf(0.0f, I20{}, I20{}, I1{});
+    if (s.NLy == 16 && s.NLz == 16) return tryf(0.0f, I16{}, I16{}, I4{}, I2{}) || tryf(0.0f, I16{}, I16{}, I2{}, I2{});
+    if (s.NLy == 16 && s.NLz == 32) return tryf(0.0f, I16{}, I32{}, I2{}, I2{}) || tryf(0.0f, I16{}, I32{}, I1{}, I2{});
+    if (s.NLy == 20 && s.NLz == 20) return tryf(0.0f, I20{}, I20{}, I2{}, I2{}) || tryf(0.0f, I20{}, I20{}, I1{}, I2{});
   } else {
-    if (s.NLy == 16 && s.NLz == 16) return tryf(0.0, I16{}, I16{}, I2{}) || tryf(0.0, I16{}, I16{}, I1{});
-    if (s.NLy == 16 && s.NLz == 32) return tryf(0.0, I16{}, I32{}, I1{});
-    if (s.NLy == 20 && s.NLz == 20) return tryf(0.0, I20{}, I20{}, I1{});
+    if (s.NLy == 16 && s.NLz == 16) return tryf(0.0, I16{}, I16{}, I2{}, I1{}) || tryf(0.0, I16{}, I16{}, I1{}, I1{});
+    if (s.NLy == 16 && s.NLz == 32) return tryf(0.0, I16{}, I32{}, I1{}, I1{});
+    if (s.NLy == 20 && s.NLz == 20) return tryf(0.0, I20{}, I20{}, I1{}, I1{});
   }
   return false;
 }
 
 bool resident_step_fits(const System& s) {
-  return res_dispatch(s, [](auto, auto, auto, auto) {});
+  return res_dispatch(s, [](auto, auto, auto, auto, auto) {});
 }
 
 // The resident form is the default (SGPU_PARAM_TAYLOR_KERNEL 0) where it measured
-// faster than the stencil passes: complex(4) orbitals on 16x16 planes (16^3 grid
-// x 64 k x 16 bands: 0.185 against 0.204 ms per step).  Elsewhere it is slower
-// (20^3 complex(4) 1.27 against 0.73 ms; 16^3 complex(8) 0.449 against 0.434 ms):
-// with one CTA per SM, the latency of the projector-table loads in each stage's
-// KB phase is not hidden behind other CTAs' work.
+// faster than the stencil passes: 16x16 planes (16^3 grid x 64 k x 16 bands:
+// complex(4) 0.181 against 0.201 ms per step, complex(8) 0.326 against 0.437 ms).
+// Elsewhere it is slower (20^3 x 2048 orbitals: complex(4) 1.27 against 0.73 ms,
+// complex(8) 1.95 against 1.47 ms): with one CTA per SM the latency of the
+// projector-table loads in each stage's KB phase is not hidden behind other CTAs'
+// work, and the 20x20 forms spill.  The step tuner measures both per shape.
 bool resident_step_default(const System& s) {
-  return s.prec == SGPU_PREC_C64 && s.NLy == 16 && s.NLz == 16 && resident_step_fits(s);
+  return s.NLy == 16 && s.NLz == 16 && resident_step_fits(s);
 }
 
 cudaError_t launch_taylor_resident(const System& s, void* zu, double dt, double* cur, void* S) {
   cudaError_t e = cudaSuccess;
-  const bool ok = res_dispatch(s, [&](auto tag, auto gy, auto gz, auto nbc) {
-    e = launch_res_t<decltype(tag), decltype(gy)::value, decltype(gz)::value, decltype(nbc)::value>(s, zu, dt, cur, S);
+  const bool ok = res_dispatch(s, [&](auto tag, auto gy, auto gz, auto nbc, auto rz) {
+    e = launch_res_t<decltype(tag), decltype(gy)::value, decltype(gz)::value, decltype(nbc)::value,
+                     decltype(rz)::value>(s, zu, dt, cur, S);
   });
   if (!ok) return cudaErrorNotSupported;
   return e;
@@ -568,11 +575,12 @@ cudaError_t launch_taylor_resident(const System& s, void* zu, double dt, double*
 
 cudaError_t prepare_resident(const System& s) {
   cudaError_t e = cudaSuccess;
-  res_dispatch(s, [&](auto tag, auto gy, auto gz, auto nbc) {
+  res_dispatch(s, [&](auto tag, auto gy, auto gz, auto nbc, auto rz) {
     using R = decltype(tag);
     constexpr int GY = decltype(gy)::value, GZ = decltype(gz)::value, NBC = decltype(nbc)::value;
-    const size_t b = res_smem<R, GY, GZ, NBC>(s);
-    if (b > 48 * 1024) e = raise_smem_limit((const void*)k_taylor_resident<R, GY, GZ, NBC>, b);
+    constexpr int RZ = decltype(rz)::value;
+    const size_t b = res_smem<R, GY, GZ, NBC, RZ>(s);
+    if (b > 48 * 1024) e = raise_smem_limit((const void*)k_taylor_resident<R, GY, GZ, NBC, RZ>, b);
   });
   return e;
 }

@@ -64,11 +64,11 @@ def test_batch_graph_matches_sequential_steps(cuda_lib, precision):
         g.close()
     for w, x in zip(want, got):
         assert _rel(x, w) <= TOL[precision]
-    # complex(4) on 16x16 planes takes the shared-memory resident step: one kernel
-    # per Taylor step; the other systems the stencil passes: 2 kernels per stage
-    # (KB term, stencil pass) +1 for the entry-wise KB field where spheres overlap,
-    # 4 stages per step; 2 x nsteps steps
-    assert counts[0] == (2 * nsteps if precision == "c64" else 2 * nsteps * 4 * 2)
+    # 16x16 planes take the shared-memory resident step: one kernel per Taylor
+    # step; the other systems the stencil passes: 2 kernels per stage (KB term,
+    # stencil pass) +1 for the entry-wise KB field where spheres overlap, 4 stages
+    # per step; 2 x nsteps steps
+    assert counts[0] == 2 * nsteps
     assert counts[1] == 2 * nsteps * 4 * 2
     assert counts[2] == 2 * nsteps * 4 * 3
 
