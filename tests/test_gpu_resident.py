@@ -90,3 +90,22 @@ def test_flag_current_matches_oracle(case, precision, kernel):
         g.hamiltonian(0.08)
         z = g.get_state()
         assert rel(g.current_RT(kcur), O.current(sysm, kcur, z)) < 1e-12
+
+
+@pytest.mark.parametrize("nb", [1, 3, 5, 7])
+@pytest.mark.parametrize("precision", ["c128", "c64"])
+def test_resident_ragged_band_groups(cuda_lib, precision, nb):
+    """Band counts that leave the last band group of a k-point partly empty
+    (complex(4) groups of 4 bands, complex(8) of 2 on 16x16 planes), with the
+    current computed in the step."""
+    sysm, kAc, vloc, zu = S.si_supercell_system((1, 1, 1), (16, 16, 16), (3, 1, 1), nb, A=(0.0, 0.0, 1e-2))
+    dt = 0.08
+    _, zproj = O.update_projector(sysm, kAc)
+    z_ref = zu if precision == "c128" else zu.astype(np.complex64).astype(np.complex128)
+    z_ref = O.hamiltonian(sysm, kAc, vloc, zproj, dt, z_ref)
+    with _gpu(sysm, kAc, vloc, zu, precision, 2) as g:
+        g.hamiltonian(dt, flag_current=True)
+        z = g.get_state()
+        assert rel(z, z_ref) < TOL[precision]
+        kcur = kAc + np.array([1e-3, 0.0, 0.0])[:, None]
+        assert rel(g.current_RT(kcur), O.current(sysm, kcur, z)) < 1e-12
