@@ -331,8 +331,10 @@ enum {
   SGPU_PARAM_PASS_FIXED = 6,  /* stencil pass, complex(4): 1 uses the compile-time plane shapes
                                  (16x16, 16x32, 20x20, 32x32 planes, 48x48 in three y-blocks: 9-plane
                                  ring, constant offsets) where they fit, 0 the generic kernel         */
-  SGPU_PARAM_CUR_FIXED = 7,   /* current and energy stencils: 1 splits each 32x32 plane over four
-                                 CTAs (48x48: six), 2 32x32 planes of the current over two, 0 the
+  SGPU_PARAM_CUR_FIXED = 7,   /* current and energy stencils on 32x32 and 48x48 planes: 1 the
+                                 current's march with two rows per thread (32x32 split over two CTAs,
+                                 48x48 over six) and the energy's over four / six CTAs, 2 the
+                                 current's march with one row per thread (four / six CTAs), 0 the
                                  generic kernels                                                     */
   SGPU_PARAM_TAYLOR_KERNEL = 8, /* Taylor step: 1 four stencil passes over all orbitals (any grid), 2
                                  the orbitals of a band group resident in one CTA's shared memory for
@@ -437,7 +439,9 @@ enum {
   SGPU_KERNEL_UVPSI = 2,        /* the Kleinman-Bylander projections of every resident orbital       */
   SGPU_KERNEL_PSI_RHO = 3,      /* the density reduction                                             */
   SGPU_KERNEL_KB_FIELD = 4,     /* the Kleinman-Bylander term at the sphere points from the projections */
-  SGPU_KERNEL_KB_TERM = 5       /* projections and KB term in one kernel, as the Taylor step runs them  */
+  SGPU_KERNEL_KB_TERM = 5,      /* projections and KB term in one kernel, as the Taylor step runs them  */
+  SGPU_KERNEL_CURRENT_STENCIL = 6, /* the current's stencil sums of every resident orbital             */
+  SGPU_KERNEL_CURRENT_PROJ = 7  /* the nonlocal current's weighted projections of every resident orbital */
 };
 
 /* Launches `kernel` reps times back to back on the handle's stream between two

@@ -274,6 +274,99 @@ __global__ void __launch_bounds__(GY / NP * GZ) k_current_march_yh(const C2<R>* 
     d[3] = v[3];
   }
 }
+// The same march with two rows per thread: thread (r, z) owns the points of rows
+// 2r and 2r+1, so row 2r+1 is a y-neighbour in registers and the four rows above
+// it are read once for both points (six shared-memory loads a point instead of
+// eight; the march is bound by shared-memory wavefronts).  Each GY x GZ plane is
+// split over NP CTAs of GY/NP rows ((GY/NP/2)*GZ threads) plus four halo rows.
+template <typename R, int GY, int GZ, int NP, int MB = 1>
+__global__ void __launch_bounds__(GY / NP / 2 * GZ, MB) k_current_march_y2(const C2<R>* __restrict__ zu, int NLx,
+                                                                      const Nab12 nab, double* __restrict__ out) {
+  constexpr int NYH = GY / NP, NT = NYH / 2 * GZ, NYZ = GY * GZ, RB = (NYH + 4) * GZ;
+  static_assert(NYH % 2 == 0 && NT % 32 == 0 && NT <= 1024 && 4 * GZ <= NT, "two rows per thread, halo by the first");
+  __shared__ double2 buf[2][RB];
+  __shared__ double sh[32 * 4];
+  const int o = blockIdx.x / NP, h = blockIdx.x - (blockIdx.x / NP) * NP, t = threadIdx.x;
+  const C2<R>* E = zu + (size_t)o * NLx * NYZ;
+  const double* nb = nab.v;
+  const int y0 = 2 * (t / GZ), z = t - (t / GZ) * GZ;                 // local rows y0, y0 + 1
+  const int own = (h * NYH + y0) * GZ + z;                            // row y0 in the plane; y0 + 1 is own + GZ
+  const int hsrc = (((h + 1) * NYH + t / GZ) % GY) * GZ + z;          // halo row of threads t < 4 GZ
+  int zo[4];                                                          // z + n in a staged row
+#pragma unroll
+  for (int n = 1; n <= 4; ++n) zo[n - 1] = (z + n) % GZ;
+  // register queues as in k_current_march_yh (plane x + m in slot (P + m) % 5)
+  double2 qa[5], qb[5];
+#pragma unroll
+  for (int m = 0; m < 5; ++m) {
+    qa[m] = to_d2(__ldg(E + (size_t)m * NYZ + own));
+    qb[m] = to_d2(__ldg(E + (size_t)m * NYZ + own + GZ));
+  }
+  C2<R> na = __ldg(E + (size_t)(5 % NLx) * NYZ + own), nb_ = __ldg(E + (size_t)(5 % NLx) * NYZ + own + GZ);
+  int xn = 6 < NLx ? 6 : 6 - NLx;
+  double v[4] = {0, 0, 0, 0};
+  int x = 0;
+  auto step = [&](auto phase) -> bool {
+    constexpr int P = decltype(phase)::value;
+    double2* pl = buf[x & 1];
+    const double2 ea = qa[P % 5], eb = qb[P % 5];
+    pl[y0 * GZ + z] = ea;
+    pl[(y0 + 1) * GZ + z] = eb;
+    if (t < 4 * GZ) pl[NYH * GZ + t] = to_d2(__ldg(E + (size_t)x * NYZ + hsrc));
+    __syncthreads();
+    v[0] = fma(ea.x, ea.x, fma(ea.y, ea.y, fma(eb.x, eb.x, fma(eb.y, eb.y, v[0]))));
+    double2 r[5];  // rows y0 + 1 .. y0 + 5 at column z
+    r[0] = eb;
+#pragma unroll
+    for (int k = 1; k < 5; ++k) r[k] = pl[(y0 + 1 + k) * GZ + z];
+    double2 sxa = make_double2(0, 0), sya = sxa, sza = sxa, sxb = sxa, syb = sxa, szb = sxa;
+#pragma unroll
+    for (int n = 1; n <= 4; ++n) {
+      const double2 xa = qa[(P + n) % 5], xb = qb[(P + n) % 5];
+      const double2 ya = r[n - 1], yb = r[n];
+      const double2 za = pl[y0 * GZ + zo[n - 1]], zb = pl[(y0 + 1) * GZ + zo[n - 1]];
+      sxa.x = fma(nb[n - 1], xa.x, sxa.x); sxa.y = fma(nb[n - 1], xa.y, sxa.y);
+      sxb.x = fma(nb[n - 1], xb.x, sxb.x); sxb.y = fma(nb[n - 1], xb.y, sxb.y);
+      sya.x = fma(nb[3 + n], ya.x, sya.x); sya.y = fma(nb[3 + n], ya.y, sya.y);
+      syb.x = fma(nb[3 + n], yb.x, syb.x); syb.y = fma(nb[3 + n], yb.y, syb.y);
+      sza.x = fma(nb[7 + n], za.x, sza.x); sza.y = fma(nb[7 + n], za.y, sza.y);
+      szb.x = fma(nb[7 + n], zb.x, szb.x); szb.y = fma(nb[7 + n], zb.y, szb.y);
+    }
+    // aimag(conjg(e) s) = e.x s.y - e.y s.x, point a then point b
+    v[1] = fma(eb.x, sxb.y, fma(-eb.y, sxb.x, fma(ea.x, sxa.y, fma(-ea.y, sxa.x, v[1]))));
+    v[2] = fma(eb.x, syb.y, fma(-eb.y, syb.x, fma(ea.x, sya.y, fma(-ea.y, sya.x, v[2]))));
+    v[3] = fma(eb.x, szb.y, fma(-eb.y, szb.x, fma(ea.x, sza.y, fma(-ea.y, sza.x, v[3]))));
+    qa[P % 5] = to_d2(na);  // plane x+5 takes the slot of plane x
+    qb[P % 5] = to_d2(nb_);
+    na = __ldg(E + (size_t)xn * NYZ + own);
+    nb_ = __ldg(E + (size_t)xn * NYZ + own + GZ);
+    xn = xn + 1 < NLx ? xn + 1 : 0;
+    ++x;
+    return x < NLx;
+  };
+  for (;;) {
+    if (!step(std::integral_constant<int, 0>{})) break;
+    if (!step(std::integral_constant<int, 1>{})) break;
+    if (!step(std::integral_constant<int, 2>{})) break;
+    if (!step(std::integral_constant<int, 3>{})) break;
+    if (!step(std::integral_constant<int, 4>{})) break;
+  }
+  block_sum<4>(v, sh);
+  if (t == 0) {
+    double* d = out + 4 * (size_t)blockIdx.x;
+    d[0] = v[0];
+    d[1] = v[1];
+    d[2] = v[2];
+    d[3] = v[3];
+  }
+}
+template <typename R, int GY, int GZ, int NP, int MB = 1>
+static cudaError_t current_march_y2(System& s, const Nab12& nab, double* out) {
+  k_current_march_y2<R, GY, GZ, NP, MB><<<NP * s.norb, GY / NP / 2 * GZ, 0, s.launch_stream()>>>((const C2<R>*)s.zu,
+                                                                                             s.NLx, nab, out);
+  return cudaGetLastError();
+}
+
 template <typename R, int GY, int GZ, int NP>
 static cudaError_t current_march_yh(System& s, const Nab12& nab, double* out) {
   k_current_march_yh<R, GY, GZ, NP><<<NP * s.norb, GY / NP * GZ, 0, s.launch_stream()>>>((const C2<R>*)s.zu, s.NLx,
@@ -348,18 +441,25 @@ __global__ void __launch_bounds__(256, 2) k_current_plane(const C2<R>* __restric
 // psi(J(j)) is read from src[o*ld + idx[j]]: the compact sphere values S with
 // the sphere-point map qmap when they are current, else the orbitals with the
 // grid index idx_proj.
-// One CTA per (projector item, k-point) and group of up to 32 bands of that
-// k-point computes the complex product C[band][p,w] = sum_j psi_b(j) B_j[p,w],
-// B_j[p,w] = conj(zproj_p(j)) r_w(j), in chunks of UVW_CH points: the chunk's B
-// (16 entries per point) and the bands' values at its points are staged in shared
-// memory (band rows padded by one element against bank conflicts); thread (tile,
-// part) accumulates a tile of 4 bands x the 4 weights of one projector over every
-// eighth point in FP64, and the eight parts are added in a fixed order.
+// One CTA per (projector item, k-point, group of up to 32 bands of that k-point,
+// part of the item's points): the points are split into nsplit contiguous ranges
+// of UVW_CH-point chunks so that the grid fills the GPU, and each range writes its
+// own partial Uw[part][o][ilma][w] (k_current_comb adds the parts in order).  Per
+// chunk, conj(zproj) of the item's projectors, the weights r and the bands' values
+// are staged in shared memory (band rows padded by one element: the eight band
+// rows a warp reads at one point fall in distinct banks).  Thread (lane, warp)
+// takes bands bg, bg+8, bg+16, bg+24 (bg = lane & 7) of projector lane >> 3 over
+// every eighth point of the chunk: t = conj(zproj) psi once, then
+// Uw[., 0] += t, Uw[., w] += r_w t (12 FP64 operations a band and point instead
+// of the 16 of four complex products), and the eight warps' sums are added in
+// a fixed order.
 constexpr int UVW_CH = 128;
 template <typename R> struct UvwGeom {
   static constexpr int SROW = UVW_CH + 1;  // padded band row
-  static constexpr size_t smem =
-      sizeof(C2<R>) * 32 * SROW + sizeof(double2) * 16 * UVW_CH + sizeof(int) * UVW_CH;
+  static constexpr size_t stage = sizeof(C2<R>) * 32 * SROW + sizeof(double2) * 4 * UVW_CH +
+                                  sizeof(double) * 3 * UVW_CH + sizeof(int) * UVW_CH;
+  static constexpr size_t red = sizeof(double2) * 8 * 32 * 9;  // the part sums, eight entries (+1 pad) at a time
+  static constexpr size_t smem = stage > red ? stage : red;
 };
 
 template <typename R>
@@ -367,45 +467,45 @@ __global__ void __launch_bounds__(256, 2) k_uvpsi_w(const C2<R>* __restrict__ sr
                                                      const double2* __restrict__ zproj, int Nlma, int Nps,
                                                      const int* __restrict__ idx, const int* __restrict__ atom_off,
                                                      const double* __restrict__ rpos, const int4* __restrict__ items,
-                                                     const int* __restrict__ lma_list, double2* __restrict__ Uw) {
+                                                     const int* __restrict__ lma_list, int nsplit, int norb,
+                                                     double2* __restrict__ Uw) {
   constexpr int CH = UVW_CH, SROW = UvwGeom<R>::SROW;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C2<R>* ps = reinterpret_cast<C2<R>*>(smem_raw);                          // [32][SROW] band values
-  double2* Bs = reinterpret_cast<double2*>(ps + 32 * SROW);                 // [CH][16] weighted rows
-  int* is = reinterpret_cast<int*>(Bs + 16 * CH);                          // [CH] gather index
-  double2* red = reinterpret_cast<double2*>(smem_raw);                     // [8][32][16] after the sums
+  double2* cz = reinterpret_cast<double2*>(ps + 32 * SROW);                // [4][CH] conj(zproj)
+  double* rw = reinterpret_cast<double*>(cz + 4 * CH);                     // [CH][3] weights x, y, z
+  int* is = reinterpret_cast<int*>(rw + 3 * CH);                           // [CH] gather index
+  double2* red = reinterpret_cast<double2*>(smem_raw);                     // [8][32][9] after the sums
   const int t = threadIdx.x, lane = t & 31, part = t >> 5;
-  const int bg = lane & 7, pg = lane >> 3;  // bands 4bg..4bg+3, projector pg (its 4 weights)
+  const int bg = lane & 7, pg = lane >> 3;  // bands bg + 8i, projector pg (its 4 weights)
   const int4 item = items[blockIdx.x];
-  const int kl = blockIdx.y, b0 = blockIdx.z * 32;
+  const int kl = blockIdx.y, b0 = (blockIdx.z / nsplit) * 32, split = blockIdx.z - (blockIdx.z / nsplit) * nsplit;
   const int a = item.x, l0 = item.y, np = item.z;
   const int p0 = atom_off[a], mps = atom_off[a + 1] - p0;
   const int nbr = min(32, NBocc - b0);
   if (nbr <= 0) return;  // whole CTA leaves together
+  const int nch = (mps + CH - 1) / CH, cps = (nch + nsplit - 1) / nsplit;
+  const int cbeg = min(nch, split * cps), cend = min(nch, cbeg + cps);  // may be empty: zeros are written
   double2 acc[4][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int w = 0; w < 4; ++w) acc[i][w] = make_double2(0.0, 0.0);
-  for (int c0 = 0; c0 < mps; c0 += CH) {
-    const int len = min(CH, mps - c0);
+  for (int c = cbeg; c < cend; ++c) {
+    const int c0 = c * CH, len = min(CH, mps - c0);
     __syncthreads();  // the previous chunk is no longer read
-    for (int q = t; q < 4 * CH; q += 256) {  // B of point j, projector p
+    for (int q = t; q < 4 * CH; q += 256) {  // conj(zproj) of point j, projector p
       const int p = q / CH, j = q - p * CH;
       double2 z = make_double2(0.0, 0.0);
-      double r1 = 0.0, r2 = 0.0, r3 = 0.0;
-      if (j < len && p < np) {
-        z = zproj[((size_t)kl * Nlma + lma_list[l0 + p]) * Nps + c0 + j];
+      if (j < len && p < np) z = zproj[((size_t)kl * Nlma + lma_list[l0 + p]) * Nps + c0 + j];
+      cz[p * CH + j] = make_double2(z.x, -z.y);
+      if (p == 0) {
         const double* r = rpos + 3 * (size_t)(p0 + c0 + j);
-        r1 = r[0]; r2 = r[1]; r3 = r[2];
+        rw[3 * j] = j < len ? r[0] : 0.0;
+        rw[3 * j + 1] = j < len ? r[1] : 0.0;
+        rw[3 * j + 2] = j < len ? r[2] : 0.0;
+        is[j] = j < len ? idx[p0 + c0 + j] : 0;
       }
-      const double2 cz = make_double2(z.x, -z.y);  // conj(zproj)
-      double2* bd = Bs + j * 16 + 4 * p;
-      bd[0] = cz;
-      bd[1] = make_double2(cz.x * r1, cz.y * r1);
-      bd[2] = make_double2(cz.x * r2, cz.y * r2);
-      bd[3] = make_double2(cz.x * r3, cz.y * r3);
-      if (p == 0 && j < len) is[j] = idx[p0 + c0 + j];
     }
     __syncthreads();
     const int tot = 32 * len;
@@ -428,45 +528,50 @@ __global__ void __launch_bounds__(256, 2) k_uvpsi_w(const C2<R>* __restrict__ sr
     }
     __syncthreads();
     for (int j = part; j < len; j += 8) {
-      double2 e[4], bw[4];
+      const double2 zc = cz[pg * CH + j];
+      const double r1 = rw[3 * j], r2 = rw[3 * j + 1], r3 = rw[3 * j + 2];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) e[i] = to_d2(ps[(4 * bg + i) * SROW + j]);
-#pragma unroll
-      for (int w = 0; w < 4; ++w) bw[w] = Bs[j * 16 + 4 * pg + w];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int w = 0; w < 4; ++w) {  // acc += e * B
-          acc[i][w].x += e[i].x * bw[w].x - e[i].y * bw[w].y;
-          acc[i][w].y += e[i].x * bw[w].y + e[i].y * bw[w].x;
-        }
+      for (int i = 0; i < 4; ++i) {
+        const double2 e = to_d2(ps[(bg + 8 * i) * SROW + j]);
+        const double tx = fma(zc.x, e.x, -zc.y * e.y), ty = fma(zc.x, e.y, zc.y * e.x);
+        acc[i][0].x += tx;
+        acc[i][0].y += ty;
+        acc[i][1].x = fma(r1, tx, acc[i][1].x);
+        acc[i][1].y = fma(r1, ty, acc[i][1].y);
+        acc[i][2].x = fma(r2, tx, acc[i][2].x);
+        acc[i][2].y = fma(r2, ty, acc[i][2].y);
+        acc[i][3].x = fma(r3, tx, acc[i][3].x);
+        acc[i][3].y = fma(r3, ty, acc[i][3].y);
+      }
     }
   }
-  __syncthreads();  // the staging buffers are reused for the part sums
+  // the eight warps' sums, eight of a thread's sixteen entries at a time
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int half = 0; half < 2; ++half) {
+    __syncthreads();  // the staging buffers (or the previous half) are no longer read
 #pragma unroll
-    for (int w = 0; w < 4; ++w) red[(part * 32 + lane) * 16 + 4 * i + w] = acc[i][w];
-  __syncthreads();
-  for (int q = t; q < 32 * 16; q += 256) {  // (tile, entry): sum the 8 parts in order
-    const int tile = q >> 4, k = q & 15;
-    double2 sum = make_double2(0.0, 0.0);
+    for (int k = 0; k < 8; ++k) red[(part * 32 + lane) * 9 + k] = acc[2 * half + k / 4][k % 4];
+    __syncthreads();
+    {  // thread (lane', k): entry k of lane' summed over the parts in order
+      const int ln = t >> 3, k = t & 7;
+      double2 sum = make_double2(0.0, 0.0);
 #pragma unroll
-    for (int pp = 0; pp < 8; ++pp) {
-      const double2 v = red[(pp * 32 + tile) * 16 + k];
-      sum.x += v.x;
-      sum.y += v.y;
+      for (int pp = 0; pp < 8; ++pp) {
+        const double2 v = red[(pp * 32 + ln) * 9 + k];
+        sum.x += v.x;
+        sum.y += v.y;
+      }
+      const int tb = ln & 7, tp = ln >> 3, i = 2 * half + k / 4, w = k & 3;
+      const int b = tb + 8 * i;
+      if (tp < np && b < nbr)
+        Uw[(((size_t)split * norb + kl * NBocc + b0 + b) * Nlma + lma_list[l0 + tp]) * 4 + w] = sum;
     }
-    const int tb = tile & 7, tp = tile >> 3, i = k >> 2, w = k & 3;
-    const int b = 4 * tb + i;
-    if (tp < np && b < nbr)
-      Uw[((size_t)(kl * NBocc + b0 + b) * Nlma + lma_list[l0 + tp]) * 4 + w] = sum;
   }
 }
 
 // Per orbital, combines the plane sums and the weighted projections exactly as
 // current() does (current.f90:182-273): jo[o][d].
-__global__ void k_current_comb(const double* __restrict__ part, int nx, const double2* __restrict__ Uw,
+__global__ void k_current_comb(const double* __restrict__ part, int nx, const double2* __restrict__ Uw, int nsplit,
                                const double* __restrict__ occ_o, const double* __restrict__ kAc,
                                const int* __restrict__ iuV, int norb, int NBocc, int Nlma, double Hxyz,
                                double IaLxyz, double* __restrict__ jo) {
@@ -485,7 +590,16 @@ __global__ void k_current_comb(const double* __restrict__ part, int nx, const do
   for (int d = 0; d < 3; ++d) j[d] = occ * kAc[3 * kl + d] * v[0] + 2.0 * v[1 + d] * occ;
   double jn[3] = {0, 0, 0};
   for (int l = 0; l < Nlma; ++l) {
-    const double2* u = Uw + ((size_t)o * Nlma + l) * 4;
+    double2 u[4];  // the point-range parts of k_uvpsi_w, added in order
+#pragma unroll
+    for (int w = 0; w < 4; ++w) u[w] = Uw[((size_t)o * Nlma + l) * 4 + w];
+    for (int sp = 1; sp < nsplit; ++sp)
+#pragma unroll
+      for (int w = 0; w < 4; ++w) {
+        const double2 v = Uw[(((size_t)sp * norb + o) * Nlma + l) * 4 + w];
+        u[w].x += v.x;
+        u[w].y += v.y;
+      }
     const double f = Hxyz * (double)iuV[l];
     const double2 u0 = make_double2(u[0].x * f, u[0].y * f);
 #pragma unroll
@@ -542,17 +656,25 @@ template <typename R>
 static cudaError_t current_stencil(System& s, const Nab12& nab, const double* nab12, double* part, int& nx) {
   const int NYZ = s.NLy * s.NLz;
   nx = 1;
-  // 32x32 planes: four CTAs of 8 rows per orbital plane (value 2: two of 16 rows).
-  // sgpu_current at 32^3 x 2048 orbitals, complex(4): 0.80 ms, two parts 0.85 ms,
-  // the one-CTA x-march 0.95 ms (complex(8): 0.91 / 0.96 / 1.12 ms)
+  // 32x32 planes: two CTAs of 16 rows per orbital plane, two rows per thread at
+  // three CTAs per SM (value 2: four CTAs of 8 rows, one row per thread).
+  // At 32^3 x 2048 orbitals, complex(4): 0.328 against 0.388 ms; two rows per
+  // thread at 118 registers (two CTAs per SM) 0.709 ms, one CTA per plane 0.344 ms
+  // (complex(8): 0.394 / 0.403 / 0.642 / 0.423 ms)
   if (s.cur_fixed && s.NLy == 32 && s.NLz == 32) {
-    nx = s.cur_fixed == 2 ? 2 : 4;
-    return s.cur_fixed == 2 ? current_march_yh<R, 32, 32, 2>(s, nab, part) : current_march_yh<R, 32, 32, 4>(s, nab, part);
+    if (s.cur_fixed == 2) {
+      nx = 4;
+      return current_march_yh<R, 32, 32, 4>(s, nab, part);
+    }
+    nx = 2;
+    return current_march_y2<R, 32, 32, 2, 3>(s, nab, part);
   }
-  // 48x48 planes (the 48^3 grid): six CTAs of 8 rows (384 threads) per orbital plane
+  // 48x48 planes (the 48^3 grid): six CTAs of 8 rows per orbital plane (two rows per
+  // thread, 192 threads; value 2: one row per thread, 384 threads): 0.284 against
+  // 0.313 ms at 432 orbitals, complex(4); 0.298 against 0.328 ms complex(8)
   if (s.cur_fixed && s.NLy == 48 && s.NLz == 48) {
     nx = 6;
-    return current_march_yh<R, 48, 48, 6>(s, nab, part);
+    return s.cur_fixed == 2 ? current_march_yh<R, 48, 48, 6>(s, nab, part) : current_march_y2<R, 48, 48, 6>(s, nab, part);
   }
   if (NYZ <= 256) return current_march<R, 256, 1, 1>(s, nab, part);
   if (NYZ <= 512) return current_march<R, 512, 1, 1>(s, nab, part);
@@ -577,44 +699,55 @@ cudaError_t launch_current_stencil(System& s, double* part, int& nx) {
                                  : current_stencil<double>(s, nab, s.nab12, part, nx);
 }
 
+// The weighted projections of the nonlocal current, Uw[o][ilma][w]
+// (current.f90:225-273), from the sphere values when they are current.
+cudaError_t launch_current_proj(System& s) {
+  if (!s.Nlma || !s.nitems) return cudaSuccess;
+  cudaError_t e;
+  const size_t smem = s.prec == SGPU_PREC_C64 ? UvwGeom<float>::smem : UvwGeom<double>::smem;
+  if (smem > 48 * 1024) {  // set on every call: the attribute is per device
+    e = s.prec == SGPU_PREC_C64
+            ? cudaFuncSetAttribute(k_uvpsi_w<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+            : cudaFuncSetAttribute(k_uvpsi_w<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  const dim3 gu(s.nitems, s.nkl, (s.NBocc + 31) / 32 * s.uvw_split);
+  // the compact sphere values are current after every Taylor step: 4x fewer bytes than gathering from zu
+  const bool fromS = s.S_valid && s.Sbuf;
+  const int ld = fromS ? s.nsp : s.NL;
+  const int* idx = fromS ? s.qmap : s.idx_proj;
+  if (s.prec == SGPU_PREC_C64)
+    k_uvpsi_w<float><<<gu, 256, smem, s.launch_stream()>>>(fromS ? (const float2*)s.Sbuf : (const float2*)s.zu, ld,
+                                                            s.NBocc, s.zproj64, s.Nlma, s.Nps, idx, s.atom_off,
+                                                            s.rpos, s.items, s.lma_list, s.uvw_split, s.norb,
+                                                            s.Uw);
+  else
+    k_uvpsi_w<double><<<gu, 256, smem, s.launch_stream()>>>(fromS ? (const double2*)s.Sbuf : (const double2*)s.zu,
+                                                             ld, s.NBocc, s.zproj64, s.Nlma, s.Nps, idx, s.atom_off,
+                                                             s.rpos, s.items, s.lma_list, s.uvw_split, s.norb,
+                                                            s.Uw);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_current(System& s, double* jav_dev) {
   double* part = s.red;                              // [norb][nx][4]
   double* jo = part + (size_t)s.norb * s.NLx * 4;    // [norb][3]
   if ((size_t)s.norb * s.NLx * 4 + 3 * (size_t)s.norb + 12 > s.red_elems) return cudaErrorInvalidValue;
   int nx = 1;
   cudaError_t e;
-  if (s.cur_valid) {  // computed by the Taylor step that produced these orbitals (flag_current)
+  if (!s.cur_valid) {
+    e = launch_current_stencil(s, part, nx);
+    if (e != cudaSuccess) return e;
+  }
+  if ((e = launch_current_proj(s)) != cudaSuccess) return e;
+  if (s.cur_valid) {  // computed by the Taylor step that produced these orbitals (flag_current),
+    // on the second stream: the projections above overlap them; the sums wait here
     e = s.aux_join();
     if (e != cudaSuccess) return e;
     part = s.cur_part;
     nx = s.cur_nx;
-  } else {
-    e = launch_current_stencil(s, part, nx);
-    if (e != cudaSuccess) return e;
   }
-  if (s.Nlma && s.nitems) {
-    const size_t smem = s.prec == SGPU_PREC_C64 ? UvwGeom<float>::smem : UvwGeom<double>::smem;
-    if (smem > 48 * 1024) {  // set on every call: the attribute is per device
-      e = s.prec == SGPU_PREC_C64
-              ? cudaFuncSetAttribute(k_uvpsi_w<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-              : cudaFuncSetAttribute(k_uvpsi_w<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-    }
-    const dim3 gu(s.nitems, s.nkl, (s.NBocc + 31) / 32);
-    // the compact sphere values are current after every Taylor step: 4x fewer bytes than gathering from zu
-    const bool fromS = s.S_valid && s.Sbuf;
-    const int ld = fromS ? s.nsp : s.NL;
-    const int* idx = fromS ? s.qmap : s.idx_proj;
-    if (s.prec == SGPU_PREC_C64)
-      k_uvpsi_w<float><<<gu, 256, smem, s.launch_stream()>>>(fromS ? (const float2*)s.Sbuf : (const float2*)s.zu, ld,
-                                                              s.NBocc, s.zproj64, s.Nlma, s.Nps, idx, s.atom_off,
-                                                              s.rpos, s.items, s.lma_list, s.Uw);
-    else
-      k_uvpsi_w<double><<<gu, 256, smem, s.launch_stream()>>>(fromS ? (const double2*)s.Sbuf : (const double2*)s.zu,
-                                                               ld, s.NBocc, s.zproj64, s.Nlma, s.Nps, idx, s.atom_off,
-                                                               s.rpos, s.items, s.lma_list, s.Uw);
-  }
-  k_current_comb<<<(s.norb + 127) / 128, 128, 0, s.launch_stream()>>>(part, nx, s.Uw, s.occ_o, s.kAc_d, s.iuV_d,
+  k_current_comb<<<(s.norb + 127) / 128, 128, 0, s.launch_stream()>>>(part, nx, s.Uw, s.uvw_split, s.occ_o, s.kAc_d, s.iuV_d,
                                                                      s.norb, s.NBocc, s.Nlma, s.Hxyz, 1.0 / s.aLxyz,
                                                                      jo);
   k_current_sum<<<1, 256, 0, s.launch_stream()>>>(jo, s.norb, jav_dev);

@@ -66,14 +66,18 @@ int alloc_state_buffers(System* s) {
 bool valid(sgpu_handle h) { return h != nullptr; }
 
 // kAc(NK,3) host -> [nkl][3] device of the handle's k range
+// Host inputs go through the handle's pinned staging, so the copy is queued on
+// the stream without waiting for the work before it; the caller's array is free
+// again on return.
 int set_kac(System* s, const double* kAc) {
-  std::vector<double> loc(3 * (size_t)s->nkl);
+  if (s->kac_in_pending) CK(cudaEventSynchronize(s->ev_kac_in));  // the previous copy has read its staging
+  double* loc = s->in_h + s->NL;
   for (int kl = 0; kl < s->nkl; ++kl)
     for (int d = 0; d < 3; ++d) loc[3 * kl + d] = kAc[(size_t)d * s->NK + (s->NK_s - 1 + kl)];
   s->kAc_h.assign(kAc, kAc + 3 * (size_t)s->NK);
-  CK(cudaMemcpyAsync(s->kAc_d, loc.data(), loc.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream));
-  // the staging vector must outlive the async copy
-  CK(cudaStreamSynchronize(s->stream));
+  CK(cudaMemcpyAsync(s->kAc_d, loc, 3 * (size_t)s->nkl * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaEventRecord(s->ev_kac_in, s->stream));
+  s->kac_in_pending = true;
   return 0;
 }
 
@@ -275,7 +279,9 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
   if (e != cudaSuccess) { delete s; return cuda_fail(e, "cudaStreamCreate"); }
   if ((e = cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking)) != cudaSuccess ||
       (e = cudaEventCreateWithFlags(&s->ev_step, cudaEventDisableTiming)) != cudaSuccess ||
-      (e = cudaEventCreateWithFlags(&s->ev_cur, cudaEventDisableTiming)) != cudaSuccess)
+      (e = cudaEventCreateWithFlags(&s->ev_cur, cudaEventDisableTiming)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&s->ev_vloc_in, cudaEventDisableTiming)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&s->ev_kac_in, cudaEventDisableTiming)) != cudaSuccess)
     return bail(cuda_fail(e, "sgpu_create: second stream"));
   {
     int dev = 0;
@@ -466,7 +472,12 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
   if ((e = cudaMalloc(&s->Wbuf, (size_t)s->norb * std::max(1, s->nsp) * sizeof(double2))) != cudaSuccess)
     return bail(cuda_fail(e, "alloc W"));
   s->W_rows = (size_t)s->norb;
-  if ((e = dalloc(&s->Uw, (size_t)s->norb * std::max(1, s->Nlma) * 4)) != cudaSuccess)
+  {  // the weighted projections' point ranges: about eight CTAs per SM, at most one 128-point chunk each
+    const long ctas = std::max(1L, (long)s->nitems * s->nkl * ((s->NBocc + 31) / 32));
+    const int nch = std::max(1, (s->max_mps + 127) / 128);
+    s->uvw_split = (int)std::max(1L, std::min<long>({8L, (8L * s->nsm + ctas - 1) / ctas, (long)nch}));
+  }
+  if ((e = dalloc(&s->Uw, (size_t)s->uvw_split * s->norb * std::max(1, s->Nlma) * 4)) != cudaSuccess)
     return bail(cuda_fail(e, "alloc Uw"));
   if ((e = dalloc(&s->kAc_d, 3 * (size_t)s->nkl)) != cudaSuccess) return bail(cuda_fail(e, "alloc kAc"));
   if ((e = dalloc(&s->vloc64, s->NL)) != cudaSuccess) return bail(cuda_fail(e, "alloc vloc64"));
@@ -488,6 +499,8 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
   s->red_h_elems = (size_t)s->NL + 64;
   if ((e = cudaMallocHost((void**)&s->red_h, s->red_h_elems * sizeof(double))) != cudaSuccess)
     return bail(cuda_fail(e, "alloc pinned"));
+  if ((e = cudaMallocHost((void**)&s->in_h, ((size_t)s->NL + 3 * (size_t)s->nkl) * sizeof(double))) != cudaSuccess)
+    return bail(cuda_fail(e, "alloc pinned inputs"));
   s->stage_elems = std::max<size_t>((size_t)4 * s->NL, std::min<size_t>((size_t)1 << 22, (size_t)s->norb * s->NL));
   if ((e = dalloc(&s->stage, s->stage_elems)) != cudaSuccess) return bail(cuda_fail(e, "alloc stage"));
   // zero kAc until the caller sets one
@@ -517,6 +530,9 @@ int sgpu_destroy(sgpu_handle h) {
   if (s->gs_h) cudaFreeHost(s->gs_h);
   if (s->red_h) cudaFreeHost(s->red_h);
   if (s->aux) cudaStreamSynchronize(s->aux);
+  if (s->in_h) cudaFreeHost(s->in_h);
+  if (s->ev_vloc_in) cudaEventDestroy(s->ev_vloc_in);
+  if (s->ev_kac_in) cudaEventDestroy(s->ev_kac_in);
   if (s->stream) cudaStreamDestroy(s->stream);
   if (s->aux) cudaStreamDestroy(s->aux);
   if (s->ev_step) cudaEventDestroy(s->ev_step);
@@ -625,9 +641,12 @@ int sgpu_set_precision(sgpu_handle h, int precision) {
 int sgpu_set_vloc(sgpu_handle h, const double* vloc) {
   if (!valid(h) || !vloc) return fail(SGPU_ERR_ARG, "sgpu_set_vloc: null argument");
   System* s = h;
-  CK(cudaMemcpyAsync(s->vloc64, vloc, s->NL * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  if (s->vloc_in_pending) CK(cudaEventSynchronize(s->ev_vloc_in));  // see set_kac
+  std::memcpy(s->in_h, vloc, s->NL * sizeof(double));
+  CK(cudaMemcpyAsync(s->vloc64, s->in_h, s->NL * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaEventRecord(s->ev_vloc_in, s->stream));
+  s->vloc_in_pending = true;
   CK(sgpu::launch_r64_to_r32(s->vloc64, s->vloc32, s->NL, s->stream));
-  CK(cudaStreamSynchronize(s->stream));
   s->have_vloc = true;
   return 0;
 }
@@ -763,6 +782,7 @@ int sgpu_time_kernel(sgpu_handle h, int kernel, int reps, double* ms_per_launch)
   System* s = h;
   if (!s->have_state || !s->have_vloc || !s->have_proj)
     return fail(SGPU_ERR_STATE, "sgpu_time_kernel: state, Vloc and projectors must be set first");
+  CK(s->aux_join());  // nothing of a flag_current step still runs beside the timed launches
   sgpu::PassIO io;
   io.zc[1] = -1e-3;
   cudaEvent_t e0, e1;
@@ -785,6 +805,16 @@ int sgpu_time_kernel(sgpu_handle h, int kernel, int reps, double* ms_per_launch)
         return sgpu::launch_psi_rho(*s, (double*)s->stage);
       case SGPU_KERNEL_KB_TERM:  // projections from S and the KB field in one kernel (as in the Taylor step)
         return sgpu::launch_kb_term(*s, s->zu, true, 0, s->norb, s->NBocc, s->Wbuf);
+      case SGPU_KERNEL_CURRENT_STENCIL: {  // into the reduction scratch, not cur_part
+        int nx = 1;
+        return sgpu::launch_current_stencil(*s, s->red, nx);
+      }
+      case SGPU_KERNEL_CURRENT_PROJ: {  // from the sphere values, as after a Taylor step
+        s->S_valid = s->Sbuf != nullptr;
+        const cudaError_t e = sgpu::launch_current_proj(*s);
+        s->S_valid = false;
+        return e;
+      }
       default:
         return cudaErrorInvalidValue;
     }

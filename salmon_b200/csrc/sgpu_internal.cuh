@@ -157,13 +157,20 @@ struct System {
   void* Sbuf = nullptr;            // [norb][nsp] orbital values at the sphere points
   bool S_valid = false;            // Sbuf holds the sphere values of the resident zu
   double2* U = nullptr;            // [norb][Nlma] projections <uV e^{ikr}|psi> (scaled)
-  double2* Uw = nullptr;           // [norb][Nlma][4] weighted projections for the current
+  double2* Uw = nullptr;           // [uvw_split][norb][Nlma][4] weighted projections for the current
+  int uvw_split = 1;               // point-range parts of the weighted projections (k_uvpsi_w)
 
   // reduction scratch
   double* red = nullptr;           // device scratch for partial sums
   size_t red_elems = 0;
   double* red_h = nullptr;         // pinned host mirror
   size_t red_h_elems = 0;
+  // pinned staging of the per-step host inputs (Vloc [NL], then k+A [3*nkl]):
+  // the copies are asynchronous, and the next call waits on the event of the
+  // previous copy before it overwrites its region
+  double* in_h = nullptr;
+  cudaEvent_t ev_vloc_in = nullptr, ev_kac_in = nullptr;
+  bool vloc_in_pending = false, kac_in_pending = false;
 
   // host<->device staging for one orbital / chunked conversions
   double2* stage = nullptr;        // [stage_elems] complex(8)
@@ -192,7 +199,7 @@ struct System {
   int* sp_blk = nullptr;           // [NLx*(nyblk+1)] first sphere point of each (plane, y-block)
   int pass_tab = 1;                // stencil pass: Vloc/sphere-index tables through the ring (two-point form)
   int pass_fixed = 1;              // stencil pass: compile-time plane shapes with a 9-plane ring (complex(4))
-  int cur_fixed = 1;               // current stencil, 32x32 planes: 1 four CTAs per plane, 2 two, 0 one
+  int cur_fixed = 1;               // current stencil, 32x32 / 48x48 planes: 1 two rows per thread, 2 one, 0 generic
   int taylor_kernel = 0;           // Taylor step: 0 auto, 1 stencil passes, 2 the shared-memory resident kernel
   // The current's stencil sums {jt, F, G, H} of the resident orbitals, computed by a
   // Taylor step called with flag_current (RT/hamiltonian.f90:68-70): rows
@@ -297,6 +304,7 @@ cudaError_t launch_r64_to_r32(const double* src, float* dst, size_t n, cudaStrea
 cudaError_t launch_psi_rho(System& s, double* rho_dev);
 // per-orbital current terms and the final jav(3) (device)
 cudaError_t launch_current(System& s, double* jav_dev);
+cudaError_t launch_current_proj(System& s);
 // reduction scratch (doubles) that launch_current and launch_energy need
 size_t current_red_elems(int norb, int NLx);
 // per-orbital kinetic and nonlocal energies summed (device, 2 doubles)
