@@ -59,6 +59,7 @@ def parse():
     p.add_argument("--batched-steps", type=int, default=1000)
     p.add_argument("--no-large", action="store_true", help="skip the Si216 48^3 run")
     p.add_argument("--precond", action="store_true", help="also run the Si64 CG preconditioner comparison (minutes)")
+    p.add_argument("--no-precond", action="store_true", help="skip the Si8 CG preconditioner comparison")
     p.add_argument("--pass-fixed", type=int, default=1, choices=[0, 1],
                    help="stencil pass of the main leg: 1 compile-time plane shapes where they apply, 0 the generic kernel")
     p.add_argument("--profile-current", action="store_true",
@@ -68,8 +69,9 @@ def parse():
     p.add_argument("--no-si8", action="store_true", help="skip the Si8 16^3 resident-vs-passes leg")
     p.add_argument("--config5", type=int, default=0, metavar="STEPS",
                    help="also run the Si216 pulsed RT workload for STEPS steps (minutes; 5000 as configured)")
-    p.add_argument("--kb-kernel", type=int, default=0, choices=[0, 1, 2],
-                   help="KB term kernel of the main leg: 0 by grid size, 1 band-group tile, 2 band-quad (profiling)")
+    p.add_argument("--kb-kernel", type=int, default=0, choices=[0, 1, 2, 3],
+                   help="KB term kernel of the main leg: 0 by grid size, 1 band-group tile, 2 band-quad, "
+                        "3 split projections + point-parallel field (profiling)")
     return p.parse_args()
 
 
@@ -320,16 +322,29 @@ def large_bench(nsteps=10):
     return out
 
 
-def precond_bench(max_outer=60):
-    """CG to a 1e-8 residual on the Si64 ground-state shape (2x2x2 diamond
-    supercell, 32^3 grid, 2x2x2 k-points, 128 occupied + 16 empty bands, fixed
-    V_loc, FP64): the learned preconditioner, trained on residual/correction
-    pairs from plain CG on one displaced configuration (sigma = 0.05 bohr),
-    evaluated on another, against TPA alone and plain CG (capped at
-    `max_outer` iterations)."""
+PRECOND_SHAPES = {
+    # the configured Si64 ground state: 2x2x2 diamond supercell, 32^3 grid, 2x2x2
+    # k-points, 128 occupied + 16 empty bands (minutes: bench.py --precond)
+    "Si64": dict(base=dict(ncell=(2, 2, 2), grid=(32, 32, 32), nkgrid=(2, 2, 2), Nb=144, Nocc=128), nconv=128,
+                 seeds=(101, 303, 202), pairs=dict(snap_at=(10, 20, 40), bands=(0, 31, 63, 95, 127)), max_outer=60),
+    # the same comparison on the Si8 cell (16^3, 2 k-points, 8 + 4 bands): seconds,
+    # in every bench run
+    "Si8": dict(base=dict(ncell=(1, 1, 1), grid=(16, 16, 16), nkgrid=(2, 1, 1), Nb=12), nconv=8,
+                seeds=(11, 13, 12), pairs=dict(), max_outer=100),
+}
+
+
+def precond_bench(shape="Si64"):
+    """CG to a 1e-8 residual on a ground-state shape (PRECOND_SHAPES, fixed V_loc,
+    FP64): the learned preconditioner, trained on residual/correction pairs from
+    plain CG on one displaced configuration (sigma = 0.05 bohr) and selected by
+    CG cost on a second (held out; TPA alone is the fallback), evaluated on a third
+    against TPA alone and plain CG (each capped at the shape's outer iterations)."""
     from salmon_b200 import precond as P
     from salmon_b200.rt import GpuSystem
-    base = dict(ncell=(2, 2, 2), grid=(32, 32, 32), nkgrid=(2, 2, 2), Nb=144, Nocc=128)
+    cfg = PRECOND_SHAPES[shape]
+    base, nconv, max_outer = cfg["base"], cfg["nconv"], cfg["max_outer"]
+    s_train, s_val, s_eval = cfg["seeds"]
 
     def gpu(seed):
         sysm, kAc, vloc, zu = P.displaced_system(base, 0.05, seed=seed)
@@ -341,35 +356,37 @@ def precond_bench(max_outer=60):
         return sysm, g
 
     t0 = time.perf_counter()
-    sysm, g = gpu(101)
-    R, E, kidx, tb = P.cg_training_pairs(g, sysm, 128, snap_at=(10, 20, 40), bands=(0, 31, 63, 95, 127))
-    vsys, gv = gpu(303)  # held-out validation configuration
+    sysm, g = gpu(s_train)
+    R, E, kidx, tb = P.cg_training_pairs(g, sysm, nconv, **cfg["pairs"])
+    vsys, gv = gpu(s_val)  # held-out validation configuration
     zv = gv.gs_get_state()
     w, report, chosen = P.train_and_select(g, P.tpa_inputs(g, R, kidx, tb), E, P.DEFAULT_VARIANTS,
-                                           lambda wt: P.cg_cost(gv, zv, wt, max_outer=max_outer, nconv=128))
+                                           lambda wt: P.cg_cost(gv, zv, wt, max_outer=max_outer, nconv=nconv))
     gv.close()
     g.close()
     t_train = time.perf_counter() - t0
     runs = {}
     for kind in ("learned", "tpa", "plain"):
-        sysm, g = gpu(202)
+        sysm, g = gpu(s_eval)
         if kind == "learned":
             g.net_set_weights(w)
         g.set_cg_preconditioner(kind)
         t1 = time.perf_counter()
-        r = P.solve_to(g, tol=1e-8, ncg=4, max_outer=max_outer, nconv=128)
+        r = P.solve_to(g, tol=1e-8, ncg=4, max_outer=max_outer, nconv=nconv)
         runs[kind] = {"outer": r["outer"], "cg_iterations": r["cg_iterations"], "residual": r["residual"],
-                      "converged": r["converged"], "seconds": time.perf_counter() - t1, "esp": r["esp"][:, :128]}
+                      "converged": r["converged"], "seconds": time.perf_counter() - t1, "esp": r["esp"][:, :nconv]}
         g.close()
     de = float(np.abs(runs["learned"]["esp"] - runs["tpa"]["esp"]).max())
     for r in runs.values():
         r.pop("esp")
+    nk = int(np.prod(base["nkgrid"]))
     return {"runs": runs, "learned_vs_plain_iterations": runs["learned"]["cg_iterations"] / runs["plain"]["cg_iterations"],
             "learned_vs_tpa_iterations": runs["learned"]["cg_iterations"] / runs["tpa"]["cg_iterations"],
             "eigenvalue_max_abs_diff_learned_vs_tpa": de, "training_pairs": int(R.shape[0]),
             "selection": {k: list(v) for k, v in report.items()}, "chosen": chosen, "training_seconds": t_train,
-            "workload": "Si64 32^3, 8 k x (128+16) bands, fixed V_loc, CG to residual 1e-8 (plain capped at "
-                        f"{max_outer} outer iterations)"}
+            "workload": f"{shape} {base['grid'][0]}x{base['grid'][1]}x{base['grid'][2]}, {nk} k x {base['Nb']} bands "
+                        f"({nconv} converged), fixed V_loc, CG to residual 1e-8 (each run capped at {max_outer} "
+                        "outer iterations)"}
 
 
 def config5_bench(nsteps=5000, nscf=60, check_steps=500, npolish=3):
@@ -663,19 +680,14 @@ def main():
         g.close()
         del stream
 
-    prec_check = None
-    if rank == 0 and not (args.only or args.no_e2e or args.no_precision):
-        prec_check = precision_check()
-    batched = None
-    if rank == 0 and not (args.only or args.no_e2e or args.no_batched):
-        batched = batched_bench(args.batched_steps)
-    large = None
-    if rank == 0 and not (args.only or args.no_e2e or args.no_large):
-        large = large_bench()
-    si8 = None
-    if rank == 0 and not (args.only or args.no_e2e or args.no_si8):
-        si8 = si8_bench()
-    pc = precond_bench() if (rank == 0 and args.precond) else None
+    # the other workloads' legs: one GPU only (a multi-GPU run reports the k-sharded step)
+    legs = rank == 0 and world == 1 and not (args.only or args.no_e2e)
+    prec_check = precision_check() if legs and not args.no_precision else None
+    batched = batched_bench(args.batched_steps) if legs and not args.no_batched else None
+    large = large_bench() if legs and not args.no_large else None
+    si8 = si8_bench() if legs and not args.no_si8 else None
+    pc = precond_bench("Si8") if legs and not args.no_precond else None
+    pc64 = precond_bench("Si64") if rank == 0 and args.precond else None
     c5 = config5_bench(args.config5) if (rank == 0 and args.config5) else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -715,6 +727,7 @@ def main():
             "large": large,
             "si8_resident_vs_passes": si8,
             "precond": pc,
+            "precond_si64": pc64,
             "config5": c5,
             "clocks": clocks,
         }

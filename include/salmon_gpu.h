@@ -327,7 +327,9 @@ enum {
                                  from global memory one plane ahead                                   */
   SGPU_PARAM_KB_KERNEL = 5,   /* KB term of H psi: 1 band-group tile kernel (32 bands of a k-point per
                                  CTA, pipelined gathers), 2 band-quad kernel (UVPSI_SPLIT warps per
-                                 4 bands), 0 the tile kernel when its grid has >= 2 CTAs per SM       */
+                                 4 bands), 3 the tile kernel's projections over KB_SPLIT point ranges
+                                 then a point-parallel field kernel, 0 the tile kernel for
+                                 complex(4) when its grid has >= 2 CTAs per SM, else form 3          */
   SGPU_PARAM_PASS_FIXED = 6,  /* stencil pass, complex(4): 1 uses the compile-time plane shapes
                                  (16x16, 16x32, 20x20, 32x32 planes, 48x48 in three y-blocks: 9-plane
                                  ring, constant offsets) where they fit, 0 the generic kernel         */
@@ -341,8 +343,10 @@ enum {
                                  the whole step (16x16, 16x32 and 20x20 planes where they fit), 0 the
                                  resident form where it is the faster one (16x16 planes), else the
                                  passes                                                              */
-  SGPU_PARAM_NSP = 9          /* sphere points of the handle (read only): the union of the
+  SGPU_PARAM_NSP = 9,         /* sphere points of the handle (read only): the union of the
                                  projectors' points, a key of the launch-shape table              */
+  SGPU_PARAM_KB_SPLIT = 10    /* KB_KERNEL 3: point ranges of the projections, 1..8; 0 about six
+                                 CTAs per SM                                                         */
 };
 
 /* CG preconditioners.  PLAIN is the reference's CG_ompk.  TPA multiplies the
@@ -375,7 +379,8 @@ int sgpu_autotune(sgpu_handle h, int reps, int* nslab, int* split, double* ms_pe
  * (SGPU_PARAM_TAYLOR_KERNEL 2 where the resident form fits, else 1), and for
  * the stencil passes the compile-time plane shapes (SGPU_PARAM_PASS_FIXED),
  * the table staging (SGPU_PARAM_PASS_TABLES), x-slabs (SGPU_PARAM_NSLAB 1, 2,
- * 4) and the KB kernel (tile, or band quad with split 1, 2, 4, 8).  Keeps the
+ * 4) and the KB kernel (tile, split tile with its automatic point ranges, or
+ * band quad with split 1, 2, 4, 8).  Keeps the
  * fastest in the handle.  params (HOST [6], may be NULL) receives
  * {taylor_kernel, pass_fixed, pass_tables, nslab, kb_kernel, uvpsi_split};
  * ms_per_step (may be NULL) its time.  The resident orbitals are not modified.

@@ -72,7 +72,8 @@ ABI = {
 }
 
 PARAMS = {"nslab": 0, "launches": 1, "uvpsi_split": 2, "cg_precond": 3, "pass_tables": 4, "kb_kernel": 5,
-          "pass_fixed": 6, "cur_fixed": 7, "taylor_kernel": 8, "nsp": 9}
+          "pass_fixed": 6, "cur_fixed": 7, "taylor_kernel": 8, "nsp": 9,
+          "kb_split": 10}
 
 KERNELS = {"stencil_pass": 0, "taylor_stage": 1, "taylor_last": 1, "uvpsi": 2, "psi_rho": 3, "kb_field": 4, "kb_term": 5,
            "current_stencil": 6, "current_proj": 7}

@@ -457,7 +457,10 @@ struct KbtGeom {
   }
 };
 
-template <typename R>
+// UONLY: phase 1 alone over the chunk range of split blockIdx.z of nsplit, the
+// unscaled sums written to Up[split][o - o_beg][ilma] (k_kb_w adds the splits
+// in order, scales, and writes U and W).
+template <typename R, bool UONLY = false>
 __global__ void __launch_bounds__(32 * KBT_WARPS * KBT_KS) k_kb_tile(const C2<R>* __restrict__ in, int ld_in, int o_beg, int nb,
                                                           int nbk, int kl0, int ngrp, const double2* __restrict__ zproj,
                                                           int Nlma, int Nps, const int* __restrict__ idx,
@@ -465,7 +468,8 @@ __global__ void __launch_bounds__(32 * KBT_WARPS * KBT_KS) k_kb_tile(const C2<R>
                                                           const int4* __restrict__ items,
                                                           const int* __restrict__ lma_list, const int* __restrict__ iuV,
                                                           double scale, double2* __restrict__ U, int nsp,
-                                                          C2<R>* __restrict__ W) {
+                                                          C2<R>* __restrict__ W, int nsplit = 1,
+                                                          double2* __restrict__ Up = nullptr) {
   using T = C2<R>;
   constexpr int CP = KbtGeom<R>::CP, SROW = KbtGeom<R>::SROW, ZROW = KbtGeom<R>::ZROW;
   constexpr int NT = 32 * KBT_WARPS * KBT_KS;
@@ -490,10 +494,14 @@ __global__ void __launch_bounds__(32 * KBT_WARPS * KBT_KS) k_kb_tile(const C2<R>
   const int4 item = items[blockIdx.y];
   const int a = item.x, l0 = item.y, np = item.z;
   const int p0 = atom_off[a], mps = atom_off[a + 1] - p0;
-  const int nch = (mps + CP - 1) / CP;
-  for (int j = t; j < mps; j += NT) {
+  const int nch_all = (mps + CP - 1) / CP;
+  // chunks [cbeg, nch) of this CTA (UONLY: its split's range, possibly empty)
+  const int cps = UONLY ? (nch_all + nsplit - 1) / nsplit : nch_all;
+  const int cbeg = UONLY ? min(nch_all, (int)blockIdx.z * cps) : 0;
+  const int nch = UONLY ? min(nch_all, cbeg + cps) : nch_all;
+  for (int j = cbeg * CP + t; j < min(mps, nch * CP); j += NT) {
     ixs[j] = __ldg(idx + p0 + j);
-    kqs[j] = __ldg(kbq + p0 + j);
+    if (!UONLY) kqs[j] = __ldg(kbq + p0 + j);
   }
   // the copy role of this thread: point jj of a chunk, for bands bc, bc + NT/CP, ...
   // and (t < 4 CP) projector pz of the zproj rows
@@ -532,8 +540,8 @@ __global__ void __launch_bounds__(32 * KBT_WARPS * KBT_KS) k_kb_tile(const C2<R>
   const int pa = n & 3, zpart = n >> 2;                    // A row n: projector n%4, Re (n<4) / Im
   const int bb = 4 * warp + (n >> 1), bpart = n & 1;       // B column n: band n/2 of the quad, Re/Im
   double c0 = 0.0, c1 = 0.0, e0 = 0.0, e1 = 0.0;
-  for (int c = 0; c < KBT_NS - 1; ++c) issue(c, true);
-  for (int c = 0; c < nch; ++c) {
+  for (int c = cbeg; c < cbeg + KBT_NS - 1; ++c) issue(c, true);
+  for (int c = cbeg; c < nch; ++c) {
     cp_async_wait<KBT_NS - 2>();  // this thread's copies of chunk c have landed
     __syncthreads();              // ... everyone's; the stage of chunk c-1 is free
     issue(c + KBT_NS - 1, true);
@@ -559,7 +567,13 @@ __global__ void __launch_bounds__(32 * KBT_WARPS * KBT_KS) k_kb_tile(const C2<R>
     }
     const double d0 = __shfl_down_sync(0xffffffffu, x0, 16);
     const double d1 = __shfl_down_sync(0xffffffffu, x1, 16);
-    if (lane < 16) {  // C rows p (Re zproj) and p+4 (Im zproj), columns of band bq
+    if (UONLY) {
+      if (lane < 16) {
+        const int p = lane >> 2, bq = lane & 3, o = o_lo + 4 * warp + bq;
+        if (p < np && o < o_hi)
+          Up[((size_t)blockIdx.z * nb + (o - o_beg)) * Nlma + lma_list[l0 + p]] = make_double2(x0 + d1, x1 - d0);
+      }
+    } else if (lane < 16) {  // C rows p (Re zproj) and p+4 (Im zproj), columns of band bq
       const int p = lane >> 2, bq = lane & 3, o = o_lo + 4 * warp + bq;
       double2 u = make_double2(0.0, 0.0);
       if (p < np && o < o_hi) {
@@ -570,6 +584,10 @@ __global__ void __launch_bounds__(32 * KBT_WARPS * KBT_KS) k_kb_tile(const C2<R>
       }
       Us[warp][p][bq] = u;
     }
+  }
+  if constexpr (UONLY) {
+    cp_async_wait<0>();
+    return;
   }
   __syncthreads();  // Us written; every warp is done with the phase-1 stages
 
@@ -630,6 +648,104 @@ static cudaError_t launch_kb_tile_t(const System& s, const void* in, int ld_in, 
   return cudaGetLastError();
 }
 
+// The KB field from the split projections: one CTA per (k-point, band group of
+// 32, projector item, KBW_T of the item's points).  The CTA adds the splits'
+// partial projections in order and scales them (the CTAs of the first point
+// range also store U for the multi-item points), then each thread takes one
+// point: its <= 4 zproj entries once, W = sum_p zproj_p U_p for every band of
+// the group, stored in sphere-point order (consecutive threads, consecutive
+// points: a warp's store is 256 contiguous bytes of one band).  The sum over p
+// runs in FP64 in projector order.
+constexpr int KBW_T = 128;
+template <typename R>
+__global__ void __launch_bounds__(KBW_T) k_kb_w(int o_beg, int nb, int nbk, int kl0, int ngrp,
+                                               const double2* __restrict__ zproj, int Nlma, int Nps,
+                                               const int* __restrict__ kbq, const int* __restrict__ atom_off,
+                                               const int4* __restrict__ items, const int* __restrict__ lma_list,
+                                               const int* __restrict__ iuV, double scale,
+                                               const double2* __restrict__ Up, int nsplit, double2* __restrict__ U,
+                                               int nsp, C2<R>* __restrict__ W) {
+  __shared__ double2 Us[KBT_BANDS][4];
+  const int t = threadIdx.x;
+  const int kq = blockIdx.x / ngrp, grp = blockIdx.x - kq * ngrp;
+  const int kl = kl0 + kq;
+  const int o_lo = max(o_beg, kl * nbk + grp * KBT_BANDS);
+  const int o_hi = min(min(o_beg + nb, (kl + 1) * nbk), kl * nbk + (grp + 1) * KBT_BANDS);
+  const int4 item = items[blockIdx.y];
+  const int a = item.x, l0 = item.y, np = item.z;
+  const int p0 = atom_off[a], mps = atom_off[a + 1] - p0;
+  if (o_lo >= o_hi || (int)blockIdx.z * KBW_T >= mps) return;  // whole CTA leaves together
+  for (int q = t; q < KBT_BANDS * 4; q += KBW_T) {
+    const int b = q >> 2, p = q & 3, o = o_lo + b;
+    double2 u = make_double2(0.0, 0.0);
+    if (p < np && o < o_hi) {
+      const int ilma = lma_list[l0 + p];
+      const double2* src = Up + (size_t)(o - o_beg) * Nlma + ilma;
+      for (int sp = 0; sp < nsplit; ++sp) {
+        const double2 v = src[(size_t)sp * nb * Nlma];
+        u.x += v.x;
+        u.y += v.y;
+      }
+      const double f = scale * (double)iuV[ilma];
+      u = make_double2(u.x * f, u.y * f);
+      if (blockIdx.z == 0) U[(size_t)(o - o_beg) * Nlma + ilma] = u;
+    }
+    Us[b][p] = u;
+  }
+  __syncthreads();
+  const int j = blockIdx.z * KBW_T + t;
+  if (j >= mps) return;
+  const int q = __ldg(kbq + p0 + j);  // sphere point; -1: in several items (k_kbfield_multi)
+  if (q < 0) return;
+  double2 z[4];
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+    z[p] = p < np ? __ldg(zproj + ((size_t)kl * Nlma + lma_list[l0 + p]) * Nps + j) : make_double2(0.0, 0.0);
+  C2<R>* Wo = W + (size_t)(o_lo - o_beg) * nsp + q;
+  const int nbq = o_hi - o_lo;
+  for (int b = 0; b < nbq; ++b) {
+    double2 w = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int p = 0; p < 4; ++p) w = cfma(z[p], Us[b][p], w);
+    Wo[(size_t)b * nsp] = mk<R>((R)w.x, (R)w.y);
+  }
+}
+
+template <typename R>
+static cudaError_t launch_kb_split_t(const System& s, const void* in, int ld_in, const int* idx, int o_beg, int nb,
+                                     int nbk, void* W) {
+  const int kl0 = o_beg / nbk, kl1 = (o_beg + nb - 1) / nbk;
+  const int ngrp = (nbk + KBT_BANDS - 1) / KBT_BANDS;
+  const size_t smem = KbtGeom<R>::smem(s.Nps);
+  if (!s.kb_smem_ok) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(s.stream, &cs);
+    if (e != cudaSuccess) return e;
+    if (cs == cudaStreamCaptureStatusNone && (e = prepare_kb(s)) != cudaSuccess) return e;
+  }
+  // point ranges: KB_SPLIT, or (0) enough for about six CTAs per SM
+  const int ctas = (kl1 - kl0 + 1) * ngrp * s.nitems;
+  int nsplit = std::max(1, std::min(s.kb_usplit > 0 ? s.kb_usplit : (6 * s.nsm + ctas - 1) / ctas, KB_USPLIT_MAX));
+  nsplit = (int)std::min<size_t>((size_t)nsplit, s.Up_rows / std::max(1, nb));  // what the partials' buffer holds
+  if (nsplit < 1) return cudaErrorInvalidValue;
+  dim3 grid((kl1 - kl0 + 1) * ngrp, s.nitems, nsplit);
+  k_kb_tile<R, true><<<grid, 32 * KBT_WARPS * KBT_KS, smem, s.launch_stream()>>>(
+      (const C2<R>*)in, ld_in, o_beg, nb, nbk, kl0, ngrp, s.zproj64, s.Nlma, s.Nps, idx, s.kbq, s.atom_off, s.items,
+      s.lma_list, s.iuV_d, s.Hxyz, s.U, s.nsp, (C2<R>*)W, nsplit, s.Up);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  dim3 gw((kl1 - kl0 + 1) * ngrp, s.nitems, (s.max_mps + KBW_T - 1) / KBW_T);
+  k_kb_w<R><<<gw, KBW_T, 0, s.launch_stream()>>>(o_beg, nb, nbk, kl0, ngrp, s.zproj64, s.Nlma, s.Nps, s.kbq,
+                                                  s.atom_off, s.items, s.lma_list, s.iuV_d, s.Hxyz, s.Up, nsplit,
+                                                  s.U, s.nsp, (C2<R>*)W);
+  e = cudaGetLastError();
+  if (e != cudaSuccess || s.n_multi == 0) return e;
+  dim3 g2((s.n_multi + 255) / 256, (nb + KU - 1) / KU);
+  k_kbfield_multi<R><<<g2, 256, 0, s.launch_stream()>>>(s.U, nb, o_beg, nbk, s.zproj64, s.Nlma, s.Nps, s.rec, s.cont,
+                                                         s.kb_multi, s.n_multi, s.nsp, (C2<R>*)W);
+  return cudaGetLastError();
+}
+
 static int kb_tile_ctas(const System& s, int o_beg, int nb, int nbk) {
   const int kl0 = o_beg / nbk, kl1 = (o_beg + nb - 1) / nbk;
   return (kl1 - kl0 + 1) * ((nbk + KBT_BANDS - 1) / KBT_BANDS) * s.nitems;
@@ -643,6 +759,8 @@ bool kb_tile_fits(const System& s) {  // dynamic + static shared memory of both 
 cudaError_t prepare_kb(const System& s) {
   cudaError_t e = raise_smem_limit((const void*)k_kb_tile<float>, KbtGeom<float>::smem(s.Nps));
   if (e == cudaSuccess) e = raise_smem_limit((const void*)k_kb_tile<double>, KbtGeom<double>::smem(s.Nps));
+  if (e == cudaSuccess) e = raise_smem_limit((const void*)k_kb_tile<float, true>, KbtGeom<float>::smem(s.Nps));
+  if (e == cudaSuccess) e = raise_smem_limit((const void*)k_kb_tile<double, true>, KbtGeom<double>::smem(s.Nps));
   s.kb_smem_ok = e == cudaSuccess;
   return e;
 }
@@ -665,7 +783,19 @@ cudaError_t launch_kb_term(const System& s, const void* in, bool from_S, int o_b
   const int ld = from_S ? s.nsp : s.NL;
   const int* idx = from_S ? s.qmap : s.idx_proj;
   const bool f = (prec < 0 ? s.prec : prec) == SGPU_PREC_C64;
-  const bool tile = kb_tile_fits(s) && (s.kb_kernel == 1 || (s.kb_kernel == 0 && kb_tile_ctas(s, o_beg, nb, nbk) >= 2 * s.nsm));
+  // auto: the tile kernel for complex(4) grids of >= 2 CTAs per SM, the split form
+  // otherwise.  Measured (B200, KB term per H application): 32^3 x 2048 orbitals
+  // complex(4) tile 0.110, split 0.115 ms; complex(8) 0.204 / 0.187 ms; 48^3 x 432
+  // 0.103 / 0.082 ms (band quad 0.134) and 0.166 / 0.124 ms; 32^3 x 8 k x 128 bands
+  // 0.059 / 0.056 ms (band quad 0.079) and 0.089 / 0.089 ms.  The split projections
+  // on the FP64 CUDA cores instead of the MMAs (lanes over points, 4 bands x 4
+  // projectors a thread) were slower at every shape (0.163, 0.119, 0.086 ms complex(4)).
+  const bool fits = kb_tile_fits(s);
+  const bool tile_first = f && kb_tile_ctas(s, o_beg, nb, nbk) >= 2 * s.nsm;
+  if (fits && (s.kb_kernel == 3 || (s.kb_kernel == 0 && !tile_first)))
+    return f ? launch_kb_split_t<float>(s, src, ld, idx, o_beg, nb, nbk, W)
+             : launch_kb_split_t<double>(s, src, ld, idx, o_beg, nb, nbk, W);
+  const bool tile = fits && (s.kb_kernel == 1 || s.kb_kernel == 0);
   if (tile)
     return f ? launch_kb_tile_t<float>(s, src, ld, idx, o_beg, nb, nbk, W)
              : launch_kb_tile_t<double>(s, src, ld, idx, o_beg, nb, nbk, W);

@@ -467,6 +467,9 @@ int sgpu_create(const sgpu_desc* d, int precision, sgpu_handle* out) {
     return bail(cuda_fail(e, "memset zproj32"));
   if ((e = dalloc(&s->U, (size_t)s->norb * std::max(1, s->Nlma))) != cudaSuccess) return bail(cuda_fail(e, "alloc U"));
   s->U_rows = (size_t)s->norb;
+  if ((e = dalloc(&s->Up, (size_t)sgpu::KB_USPLIT_MAX * s->norb * std::max(1, s->Nlma))) != cudaSuccess)
+    return bail(cuda_fail(e, "alloc Up"));
+  s->Up_rows = (size_t)sgpu::KB_USPLIT_MAX * s->norb;
   if ((e = cudaMalloc(&s->Sbuf, (size_t)s->norb * std::max(1, s->nsp) * sizeof(double2))) != cudaSuccess)
     return bail(cuda_fail(e, "alloc S"));
   if ((e = cudaMalloc(&s->Wbuf, (size_t)s->norb * std::max(1, s->nsp) * sizeof(double2))) != cudaSuccess)
@@ -521,7 +524,7 @@ int sgpu_destroy(sgpu_handle h) {
   free_state_buffers(s);
   void* bufs[] = {s->vloc64, s->vloc32, s->occ_o, s->kAc_d, s->idx_proj, s->atom_off, s->rpos, s->items,
                   s->lma_list, s->iuV_d, s->lma_atom, s->uV_d, s->zproj64, s->zproj32, s->sp_off, s->rec, s->cont, s->qmap, s->kbq, s->kb_multi, s->lqi, s->Sbuf, s->Wbuf,
-                  s->U, s->Uw, s->red, s->stage, s->cur_part, s->nab12};
+                  s->U, s->Up, s->Uw, s->red, s->stage, s->cur_part, s->nab12};
   for (void* p : bufs) cudaFree(p);
   void* gbufs[] = {s->gs_zu, s->gs_aux, s->gs_W, s->gs_st, s->gs_part, s->gs_A, s->gs_V, s->gs_w, s->gs_sweeps,
                    s->occ_gs, s->gs_out, s->gs_res, s->gs_tb, s->vpsl, s->rho_d, s->exc_d, s->sp_blk,
@@ -879,6 +882,13 @@ int gs_alloc(System* s) {
     CK(cudaMalloc(&s->U, rows * std::max(1, s->Nlma) * sizeof(double2)));
     s->U_rows = rows;
   }
+  if ((size_t)sgpu::KB_USPLIT_MAX * rows > s->Up_rows) {  // the split KB form's partial projections
+    CK(cudaStreamSynchronize(s->stream));
+    cudaFree(s->Up);
+    s->Up = nullptr;
+    CK(cudaMalloc(&s->Up, (size_t)sgpu::KB_USPLIT_MAX * rows * std::max(1, s->Nlma) * sizeof(double2)));
+    s->Up_rows = (size_t)sgpu::KB_USPLIT_MAX * rows;
+  }
   CK(cudaStreamSynchronize(s->stream));
   return 0;
 }
@@ -1136,8 +1146,12 @@ extern "C" int sgpu_set_param(sgpu_handle h, int param, int value) {
       if (sgpu::prepare_pass(*s) != cudaSuccess) return fail(SGPU_ERR_CUDA, "sgpu_set_param: pass setup failed");
       return 0;
     case SGPU_PARAM_KB_KERNEL:
-      if (value < 0 || value > 2) return fail(SGPU_ERR_ARG, "sgpu_set_param: KB kernel must be 0, 1 or 2");
+      if (value < 0 || value > 3) return fail(SGPU_ERR_ARG, "sgpu_set_param: KB kernel must be 0 to 3");
       s->kb_kernel = value;
+      return 0;
+    case SGPU_PARAM_KB_SPLIT:
+      if (value < 0 || value > sgpu::KB_USPLIT_MAX) return fail(SGPU_ERR_ARG, "sgpu_set_param: KB split must be 0 to 8");
+      s->kb_usplit = value;
       return 0;
     case SGPU_PARAM_CUR_FIXED:
       if (value < 0 || value > 2) return fail(SGPU_ERR_ARG, "sgpu_set_param: current fixed shape must be 0, 1 or 2");
@@ -1177,6 +1191,7 @@ extern "C" int sgpu_get_param(sgpu_handle h, int param, int* value) {
     case SGPU_PARAM_CUR_FIXED: *value = h->cur_fixed; return 0;
     case SGPU_PARAM_TAYLOR_KERNEL: *value = h->taylor_kernel; return 0;
     case SGPU_PARAM_NSP: *value = h->nsp; return 0;
+    case SGPU_PARAM_KB_SPLIT: *value = h->kb_usplit; return 0;
     default: return fail(SGPU_ERR_ARG, "sgpu_get_param: unknown parameter");
   }
 }
@@ -1265,9 +1280,9 @@ extern "C" int sgpu_autotune_step(sgpu_handle h, double dt, int reps, int* param
     for (int pt : {1, 0})
       for (int ns : {1, 2, 4}) {
         if (ns > 1 && s->NLx / ns < 8) continue;
-        for (int sp : {0, 1, 2, 4, 8}) {  // 0: the band-group tile kernel
-          if (sp == 0 && !sgpu::kb_tile_fits(*s)) continue;
-          cands.push_back({1, pf, pt, ns, sp ? 2 : 1, sp ? sp : old[5]});
+        for (int sp : {-1, 0, 1, 2, 4, 8}) {  // -1: the split tile, 0: the band-group tile kernel
+          if (sp <= 0 && !sgpu::kb_tile_fits(*s)) continue;
+          cands.push_back({1, pf, pt, ns, sp < 0 ? 3 : (sp ? 2 : 1), sp > 0 ? sp : old[5]});
         }
       }
   for (const auto& c : cands) {

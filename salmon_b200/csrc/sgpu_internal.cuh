@@ -11,6 +11,8 @@
 
 namespace sgpu {
 
+constexpr int KB_USPLIT_MAX = 8;  // point ranges of the split KB projections
+
 // ---------------------------------------------------------------- complex --
 template <typename R> struct C2Of;
 template <> struct C2Of<float> { using type = float2; };
@@ -224,7 +226,10 @@ struct System {
   int nsm = 148;                   // SMs of the device
   mutable bool kb_smem_ok = false;  // the KB tile kernels' shared-memory limits are raised for this handle
   int um_split = 4;                // band-quad KB kernel: warps splitting the points of one tile (1, 2, 4, 8)
-  int kb_kernel = 0;               // KB term: 0 auto, 1 band-group tile kernel, 2 band-quad kernel
+  int kb_kernel = 0;               // KB term: 0 auto, 1 band-group tile kernel, 2 band-quad kernel, 3 split tile
+  int kb_usplit = 0;               // split tile: point ranges of the projections (<= KB_USPLIT_MAX; 0 auto)
+  double2* Up = nullptr;           // [Up_rows][Nlma] partial projections of the split tile
+  size_t Up_rows = 0;
   int cg_precond = 0;              // ground-state CG preconditioner: 0 none, 1 TPA, 2 learned
   double cg_delta = 1e-15;         // CG stops a band when its Rayleigh quotient moves less than this
   bool net_ready = false;          // a preconditioner network has been loaded

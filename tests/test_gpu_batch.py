@@ -28,6 +28,7 @@ def _open(items, precision):
     gs = []
     for sysm, kAc, vloc, zu in items:
         g = GpuSystem(sysm, precision)
+        g.set_param("kb_kernel", 1)  # the tile KB kernel: a fixed launch count per stage
         g.set_state(zu)
         g.set_vloc(vloc)
         g.update_projector(kAc)

@@ -192,16 +192,21 @@ def test_pass_table_staging(case, precision, tables, nslab):
         assert rel(g.get_state(), O.hamiltonian(sysm, kAc, vloc, zproj, dt, z0)) < tol_s
 
 
-def _kb_form_checks(sysm, kAc, vloc, zu, zproj, precision, split):
+# KB term forms: the band-group tile kernel, the band-quad kernel with 4 warps a
+# quad, and the split form: the tile kernel's projections over 1 or 3 point ranges
+# followed by the field kernel
+KB_FORMS = {"tile": {"kb_kernel": 1}, "quad4": {"kb_kernel": 2, "uvpsi_split": 4},
+            "split1": {"kb_kernel": 3, "kb_split": 1}, "split3": {"kb_kernel": 3, "kb_split": 3}}
+
+
+def _kb_form_checks(sysm, kAc, vloc, zu, zproj, precision, form):
     import torch
     tol_h, tol_s = (TOL64, TOL64) if precision == "c128" else (TOL32_HPSI, TOL32_STEP)
     z0 = zu if precision == "c128" else c64_round(zu)
     with make_gpu(sysm, kAc, vloc, zu, precision) as g:
-        if split == 0:
-            g.set_param("kb_kernel", 1)
-        else:
-            g.set_param("kb_kernel", 2)
-            g.set_param("uvpsi_split", split)
+        for k, v in KB_FORMS[form].items():
+            g.set_param(k, v)
+            assert g.get_param(k) == v
         for ikl in range(sysm.nk_local):
             ik = sysm.NK_s + ikl
             t = zu[ikl, -1]
@@ -223,35 +228,35 @@ def _kb_form_checks(sysm, kAc, vloc, zu, zproj, precision, split):
         assert rel(g.get_state(), O.hamiltonian(sysm, kAc, vloc, zproj, 0.08, z0)) < tol_s
 
 
-@pytest.mark.parametrize("split", [0, 4])
+@pytest.mark.parametrize("form", list(KB_FORMS))
 @pytest.mark.parametrize("precision", ["c128", "c64"])
-def test_kb_forms(case, precision, split):
-    """The KB term of H psi by the band-group tile kernel (split 0: kb_kernel 1)
-    and by the band-quad kernel (kb_kernel 2, split 4): single orbitals, a band range that cuts k-point
-    blocks, and a Taylor step, against the oracle."""
+def test_kb_forms(case, precision, form):
+    """The KB term of H psi by each form (KB_FORMS): single orbitals, a band range
+    that cuts k-point blocks, and a Taylor step, against the oracle."""
     _, sysm, kAc, vloc, zu, zproj = case
-    _kb_form_checks(sysm, kAc, vloc, zu, zproj, precision, split)
+    _kb_form_checks(sysm, kAc, vloc, zu, zproj, precision, form)
 
 
-@pytest.mark.parametrize("split", [0, 4])
+@pytest.mark.parametrize("form", list(KB_FORMS))
 @pytest.mark.parametrize("precision", ["c128", "c64"])
-def test_kb_forms_many_bands(cuda_lib, precision, split):
+def test_kb_forms_many_bands(cuda_lib, precision, form):
     """More bands than one tile's 32 (a partial second band group) and three
     atoms whose spheres overlap."""
     sysm, kAc, vloc, zu = S.small_system(8, 10, 12, nk=2, nb=37, nat=3, seed=31, Rps=2.2)
     _, zproj = O.update_projector(sysm, kAc)
-    _kb_form_checks(sysm, kAc, vloc, zu, zproj, precision, split)
+    _kb_form_checks(sysm, kAc, vloc, zu, zproj, precision, form)
 
 
+@pytest.mark.parametrize("kb_kernel", [1, 3])
 @pytest.mark.parametrize("precision", ["c128", "c64"])
-def test_kb_tile_32cubed(cuda_lib, precision):
-    """The band-group KB kernel at a production grid (32^3, 8 atoms, ~1000
-    points per sphere: the largest shared-memory tile) against the oracle."""
+def test_kb_tile_32cubed(cuda_lib, precision, kb_kernel):
+    """The band-group KB kernel and its split form at a production grid (32^3, 8
+    atoms, ~1000 points per sphere: the largest shared-memory tile) against the oracle."""
     sysm, kAc, vloc, zu = S.microbench_system(32, nk_limit=1, Nb=8)
     _, zproj = O.update_projector(sysm, kAc)
     tol = TOL64 if precision == "c128" else TOL32_HPSI
     with make_gpu(sysm, kAc, vloc, zu, precision) as g:
-        g.set_param("kb_kernel", 1)
+        g.set_param("kb_kernel", kb_kernel)
         ik = sysm.NK_s
         for b in (0, sysm.NBoccmax - 1):
             t = zu[0, b]

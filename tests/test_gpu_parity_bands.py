@@ -5,7 +5,7 @@ the tilings that small cases never reach.
                                   hpsi/Taylor microbench's per-k-point tiling)
   32^3, one k-point x 128 bands   the Si64 supercell with the physical Si
                                   pseudopotential: four band groups; each KB
-                                  kernel form (auto, tile, band quad)
+                                  kernel form (auto, tile, band quad, split tile)
   48^3, one k-point x 432 bands   the Si216 shape: the y-block stencil pass with
                                   fourteen band groups
   batched Si8 + Si16 + Si64       one CUDA-graph replay of the three systems,
@@ -75,7 +75,7 @@ def _si64_pp():
     return sysm, kAc, vpsl, zu
 
 
-@pytest.mark.parametrize("kb_kernel", [0, 1, 2])
+@pytest.mark.parametrize("kb_kernel", [0, 1, 2, 3])
 @pytest.mark.parametrize("precision", ["c128", "c64"])
 def test_si64_pseudopotential_128_bands(cuda_lib, precision, kb_kernel):
     sysm, kAc, vloc, zu = _si64_pp()
