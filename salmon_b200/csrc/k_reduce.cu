@@ -571,25 +571,20 @@ __global__ void __launch_bounds__(256, 2) k_uvpsi_w(const C2<R>* __restrict__ sr
 
 // Per orbital, combines the plane sums and the weighted projections exactly as
 // current() does (current.f90:182-273): jo[o][d].
-__global__ void k_current_comb(const double* __restrict__ part, int nx, const double2* __restrict__ Uw, int nsplit,
-                               const double* __restrict__ occ_o, const double* __restrict__ kAc,
-                               const int* __restrict__ iuV, int norb, int NBocc, int Nlma, double Hxyz,
-                               double IaLxyz, double* __restrict__ jo) {
-  const int o = blockIdx.x * blockDim.x + threadIdx.x;
-  if (o >= norb) return;
-  double v[4] = {0, 0, 0, 0};
-  for (int x = 0; x < nx; ++x) {  // per-orbital rows of partial sums, in order
-    const double* d = part + ((size_t)o * nx + x) * 4;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) v[k] += d[k];
-  }
-  const int kl = o / NBocc;
+// One warp per orbital: lane l takes projectors l, l+32, ... in order, the lanes'
+// nonlocal sums are added by a fixed butterfly, and lane 0 adds the plane sums.
+constexpr int COMB_T = 256;
+__global__ void __launch_bounds__(COMB_T) k_current_comb(const double* __restrict__ part, int nx,
+                                                        const double2* __restrict__ Uw, int nsplit,
+                                                        const double* __restrict__ occ_o,
+                                                        const double* __restrict__ kAc, const int* __restrict__ iuV,
+                                                        int norb, int NBocc, int Nlma, double Hxyz, double IaLxyz,
+                                                        double* __restrict__ jo) {
+  const int o = blockIdx.x * (COMB_T / 32) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (o >= norb) return;  // whole warp
   const double occ = occ_o[o];
-  double j[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) j[d] = occ * kAc[3 * kl + d] * v[0] + 2.0 * v[1 + d] * occ;
   double jn[3] = {0, 0, 0};
-  for (int l = 0; l < Nlma; ++l) {
+  for (int l = lane; l < Nlma; l += 32) {
     double2 u[4];  // the point-range parts of k_uvpsi_w, added in order
 #pragma unroll
     for (int w = 0; w < 4; ++w) u[w] = Uw[((size_t)o * Nlma + l) * 4 + w];
@@ -610,7 +605,23 @@ __global__ void k_current_comb(const double* __restrict__ part, int nx, const do
     }
   }
 #pragma unroll
-  for (int d = 0; d < 3; ++d) jo[3 * (size_t)o + d] = j[d] * Hxyz * IaLxyz + jn[d];
+  for (int d = 0; d < 3; ++d)
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) jn[d] += __shfl_xor_sync(0xffffffffu, jn[d], off);
+  if (lane == 0) {
+    double v[4] = {0, 0, 0, 0};
+    for (int x = 0; x < nx; ++x) {  // per-orbital rows of partial sums, in order
+      const double* d = part + ((size_t)o * nx + x) * 4;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) v[k] += d[k];
+    }
+    const int kl = o / NBocc;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double j = occ * kAc[3 * kl + d] * v[0] + 2.0 * v[1 + d] * occ;
+      jo[3 * (size_t)o + d] = j * Hxyz * IaLxyz + jn[d];
+    }
+  }
 }
 
 // sum over orbitals in a fixed order
@@ -747,7 +758,7 @@ cudaError_t launch_current(System& s, double* jav_dev) {
     part = s.cur_part;
     nx = s.cur_nx;
   }
-  k_current_comb<<<(s.norb + 127) / 128, 128, 0, s.launch_stream()>>>(part, nx, s.Uw, s.uvw_split, s.occ_o, s.kAc_d, s.iuV_d,
+  k_current_comb<<<(s.norb + COMB_T / 32 - 1) / (COMB_T / 32), COMB_T, 0, s.launch_stream()>>>(part, nx, s.Uw, s.uvw_split, s.occ_o, s.kAc_d, s.iuV_d,
                                                                      s.norb, s.NBocc, s.Nlma, s.Hxyz, 1.0 / s.aLxyz,
                                                                      jo);
   k_current_sum<<<1, 256, 0, s.launch_stream()>>>(jo, s.norb, jav_dev);
