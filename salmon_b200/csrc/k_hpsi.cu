@@ -649,14 +649,15 @@ static cudaError_t launch_kb_tile_t(const System& s, const void* in, int ld_in, 
 }
 
 // The KB field from the split projections: one CTA per (k-point, band group of
-// 32, projector item, KBW_T of the item's points).  The CTA adds the splits'
-// partial projections in order and scales them (the CTAs of the first point
-// range also store U for the multi-item points), then each thread takes one
-// point: its <= 4 zproj entries once, W = sum_p zproj_p U_p for every band of
-// the group, stored in sphere-point order (consecutive threads, consecutive
-// points: a warp's store is 256 contiguous bytes of one band).  The sum over p
-// runs in FP64 in projector order.
-constexpr int KBW_T = 128;
+// 32, projector item, KBW_T of the item's points).  Each thread first issues the
+// loads of its point (sphere index, <= 4 zproj entries), then the CTA adds the
+// splits' partial projections in order and scales them (the CTAs of the first
+// point range also store U for the multi-item points), so both sets of loads are
+// in flight together; then W = sum_p zproj_p U_p for every band of the group,
+// stored in sphere-point order (consecutive threads, consecutive points: a warp's
+// store is 256 contiguous bytes of one band).  The sum over p runs in FP64 in
+// projector order.
+constexpr int KBW_T = 256;
 template <typename R>
 __global__ void __launch_bounds__(KBW_T) k_kb_w(int o_beg, int nb, int nbk, int kl0, int ngrp,
                                                const double2* __restrict__ zproj, int Nlma, int Nps,
@@ -675,8 +676,16 @@ __global__ void __launch_bounds__(KBW_T) k_kb_w(int o_beg, int nb, int nbk, int 
   const int a = item.x, l0 = item.y, np = item.z;
   const int p0 = atom_off[a], mps = atom_off[a + 1] - p0;
   if (o_lo >= o_hi || (int)blockIdx.z * KBW_T >= mps) return;  // whole CTA leaves together
-  for (int q = t; q < KBT_BANDS * 4; q += KBW_T) {
-    const int b = q >> 2, p = q & 3, o = o_lo + b;
+  const int j = blockIdx.z * KBW_T + t;
+  // this thread's point: sphere index (-1: in several items, k_kbfield_multi) and zproj
+  const int q = j < mps ? __ldg(kbq + p0 + j) : -1;
+  double2 z[4];
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+    z[p] = (p < np && j < mps) ? __ldg(zproj + ((size_t)kl * Nlma + lma_list[l0 + p]) * Nps + j)
+                               : make_double2(0.0, 0.0);
+  for (int i = t; i < KBT_BANDS * 4; i += KBW_T) {
+    const int b = i >> 2, p = i & 3, o = o_lo + b;
     double2 u = make_double2(0.0, 0.0);
     if (p < np && o < o_hi) {
       const int ilma = lma_list[l0 + p];
@@ -693,16 +702,10 @@ __global__ void __launch_bounds__(KBW_T) k_kb_w(int o_beg, int nb, int nbk, int 
     Us[b][p] = u;
   }
   __syncthreads();
-  const int j = blockIdx.z * KBW_T + t;
-  if (j >= mps) return;
-  const int q = __ldg(kbq + p0 + j);  // sphere point; -1: in several items (k_kbfield_multi)
   if (q < 0) return;
-  double2 z[4];
-#pragma unroll
-  for (int p = 0; p < 4; ++p)
-    z[p] = p < np ? __ldg(zproj + ((size_t)kl * Nlma + lma_list[l0 + p]) * Nps + j) : make_double2(0.0, 0.0);
   C2<R>* Wo = W + (size_t)(o_lo - o_beg) * nsp + q;
   const int nbq = o_hi - o_lo;
+#pragma unroll 4
   for (int b = 0; b < nbq; ++b) {
     double2 w = make_double2(0.0, 0.0);
 #pragma unroll
@@ -785,9 +788,9 @@ cudaError_t launch_kb_term(const System& s, const void* in, bool from_S, int o_b
   const bool f = (prec < 0 ? s.prec : prec) == SGPU_PREC_C64;
   // auto: the tile kernel for complex(4) grids of >= 2 CTAs per SM, the split form
   // otherwise.  Measured (B200, KB term per H application): 32^3 x 2048 orbitals
-  // complex(4) tile 0.110, split 0.115 ms; complex(8) 0.204 / 0.187 ms; 48^3 x 432
-  // 0.103 / 0.082 ms (band quad 0.134) and 0.166 / 0.124 ms; 32^3 x 8 k x 128 bands
-  // 0.059 / 0.056 ms (band quad 0.079) and 0.089 / 0.089 ms.  The split projections
+  // complex(4) tile 0.112, split 0.111 ms; complex(8) 0.205 / 0.184 ms; 48^3 x 432
+  // 0.102 / 0.079 ms (band quad 0.134) and 0.164 / 0.121 ms; 32^3 x 8 k x 128 bands
+  // 0.058 / 0.055 ms (band quad 0.079) and 0.089 / 0.087 ms.  The split projections
   // on the FP64 CUDA cores instead of the MMAs (lanes over points, 4 bands x 4
   // projectors a thread) were slower at every shape (0.163, 0.119, 0.086 ms complex(4)).
   const bool fits = kb_tile_fits(s);
