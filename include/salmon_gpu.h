@@ -145,7 +145,10 @@ int sgpu_get_state(sgpu_handle h, double* zu /* complex(8), HOST */);
  * precision), layout zu(NL,NBoccmax,NK_s:NK_e). */
 void* sgpu_state_ptr(sgpu_handle h);
 
-/* HOST Vloc(NL) -> device.  Vloc = Vh + Vpsl + Vexc (RT/dt_evolve.f90:206). */
+/* HOST Vloc(NL) -> device.  Vloc = Vh + Vpsl + Vexc (RT/dt_evolve.f90:206).
+ * The values are copied into the handle's pinned staging before the call returns
+ * (the caller's array is free again); the device copy is queued on the handle's
+ * stream without waiting for the work before it. */
 int sgpu_set_vloc(sgpu_handle h, const double* vloc);
 
 /* HOST Vpsl(NL) -> device: the local pseudopotential that sgpu_update_vloc
@@ -188,7 +191,8 @@ int sgpu_vloc_extrapolate(sgpu_handle h);
 
 /* Sets k+A(t) for the following hpsi/hamiltonian calls and rebuilds the
  * k-dependent projectors zproj(j,ilma,ik) = conj(exp(i kAc.r)) uV(j,ilma).
- * kAc is HOST (NK,3).  Replaces update_projector(kac) (common/projector.f90:29-115). */
+ * kAc is HOST (NK,3), staged like sgpu_set_vloc's input (no stream wait).
+ * Replaces update_projector(kac) (common/projector.f90:29-115). */
 int sgpu_update_projector(sgpu_handle h, const double* kAc);
 
 /* One 4th-order Taylor step of every resident orbital:
