@@ -700,7 +700,7 @@ def main():
             cpu = {"unavailable": str(exc)}
     if rank == 0 and (args.only or args.no_e2e):
         print(json.dumps({p: {k: v for k, v in r.items() if k != "e2e"} for p, r in res.items()} |
-                         ({"config5": c5} if c5 else {})))
+                         ({"config5": c5} if c5 else {}) | ({"precond_si64": pc64} if pc64 else {})))
     elif rank == 0:
         h = res["c64"]
         tpo = NCU_TRAFFIC_BYTES_PER_ORBITAL.get(("taylor_stage", "c64", args.grid))
